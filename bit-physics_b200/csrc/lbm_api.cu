@@ -1,0 +1,842 @@
+// lbm_api.cu -- the C ABI of include/lbm_d3q19.h: lattice handles, state
+// transfer, the step loop and the stateless reference functions.
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "lbm_d3q19.h"
+#include "lbm_launch.h"
+
+using namespace lbm;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what)
+{
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        return fail(LBM_ERR_NOMEM, "%s: %s", what, cudaGetErrorString(e));
+    }
+    return fail(LBM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(call, what)                                   \
+    do {                                                 \
+        cudaError_t e_ = (call);                         \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+size_t storage_bytes(int storage)
+{
+    switch (storage) {
+    case LBM_STORAGE_F64: return 8;
+    case LBM_STORAGE_F32: return 4;
+    case LBM_STORAGE_F16_SHIFT:
+    case LBM_STORAGE_BF16_SHIFT: return 2;
+    default: return 0;
+    }
+}
+
+// Host f64 constants with the reference's expressions (constants.py:50-57,
+// d3q19_warp.py:51-54).  volatile keeps them runtime IEEE operations.
+void fill_constants(Params& P)
+{
+    volatile double one = 1.0, two = 2.0, three = 3.0, eighteen = 18.0, thirtysix = 36.0;
+    P.cs2 = one / three;
+    P.inv_cs2 = one / P.cs2;
+    P.inv_cs4 = one / (P.cs2 * P.cs2);
+    P.inv_two_cs4 = one / (two * P.cs2 * P.cs2);
+    P.inv_two_cs2 = one / (two * P.cs2);
+    P.w[0] = one / three;
+    for (int i = 1; i <= 6; ++i) P.w[i] = one / eighteen;
+    for (int i = 7; i < Q; ++i) P.w[i] = one / thirtysix;
+}
+
+void init_geometry(Params& P, int nx, int ny, int nz)
+{
+    std::memset(&P, 0, sizeof(P));
+    P.nx = nx;
+    P.ny = ny;
+    P.nz = nz;
+    P.n = nx * ny * nz;
+    P.nynz = ny * nz;
+    P.div_nz.init((uint32_t)nz);
+    P.div_ny.init((uint32_t)ny);
+    P.periodic = 7;
+    P.wall_sum_pairwise = (long long)nx * nz == 1;
+    fill_constants(P);
+    P.tau = 1.0;
+}
+
+bool dims_ok(long long nx, long long ny, long long nz)
+{
+    if (nx < 1 || ny < 1 || nz < 1) return false;
+    long long n = nx * ny * nz;
+    return n < (1LL << 31) / 1 && n * 1 > 0;
+}
+
+}  // namespace
+
+struct lbm_lattice {
+    lbm_desc desc{};
+    int storage = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int n = 0;
+    size_t elem = 0;
+    void* buf[2] = {nullptr, nullptr};
+    int cur = 0;
+    bool pre = true;
+    uint8_t* flags = nullptr;
+    bool has_flags = false;
+    void* force = nullptr;   // (3, n) double (f64 storage) or float
+    float* poro = nullptr;   // (n)
+    void* rho = nullptr;     // readback buffers, double (f64 storage) or float
+    void* u = nullptr;
+    double* partials = nullptr;
+    double* sums = nullptr;  // 5 doubles
+    int partial_blocks = 0;
+    double* staging = nullptr; // (19, n) f64, allocated on first use
+    int64_t steps = 0;
+    int block = 256;
+    Params P{};
+};
+
+namespace {
+
+void rebuild_params(lbm_lattice* h)
+{
+    Params& P = h->P;
+    const lbm_desc& d = h->desc;
+    init_geometry(P, d.nx, d.ny, d.nz);
+    P.periodic = d.periodic & 7;
+    P.has_flags = h->has_flags ? 1 : 0;
+    P.flags = h->flags;
+    P.force = h->force;
+    P.porosity = h->poro;
+    P.tau = d.tau;
+    for (int f = 0; f < 6; ++f)
+        for (int a = 0; a < 3; ++a) {
+            P.wall_u[f][a] = d.wall_velocity[f][a];
+            P.wall_uf[f][a] = (float)d.wall_velocity[f][a];
+        }
+    for (int a = 0; a < 3; ++a) {
+        P.body_force[a] = d.body_force[a];
+        P.body_force_f[a] = (float)d.body_force[a];
+    }
+    P.drag_k = d.drag_k;
+    P.drag_kf = (float)d.drag_k;
+    // Inflow equilibrium, reciprocal form of equilibrium.py:310-322.
+    const double ux = d.inflow_u[0], uy = d.inflow_u[1], uz = d.inflow_u[2];
+    const double u_sq = ux * ux + uy * uy + uz * uz;
+    for (int q = 0; q < Q; ++q) {
+        double cu = (double)cx(q) * ux + (double)cy(q) * uy + (double)cz(q) * uz;
+        P.inflow_f[q] = P.w[q] * d.inflow_rho *
+                        (1.0 + cu * P.inv_cs2 + cu * cu * P.inv_two_cs4 - u_sq * P.inv_two_cs2);
+        P.inflow_h[q] = (float)(P.inflow_f[q] - P.w[q]);
+    }
+    P.omega = (float)(1.0 / d.tau);
+    P.pref = (float)(1.0 - 0.5 / d.tau);
+}
+
+cudaError_t launch(lbm_lattice* h, int kernel, const void* src, void* dst, bool post, double* f_out, void* rho,
+                   void* u, double* partials)
+{
+    LaunchArgs a;
+    a.P = h->P;
+    a.src = src;
+    a.dst = dst;
+    a.post = post;
+    a.f_out = f_out;
+    a.rho = rho;
+    a.u = u;
+    a.partials = partials;
+    a.block = h->block;
+    a.stream = h->stream;
+    if (h->storage == LBM_STORAGE_F64) return launch_exact(kernel, h->desc.force_mode, a);
+    return launch_fast(h->storage, kernel, h->desc.force_mode, a);
+}
+
+int ensure_staging(lbm_lattice* h)
+{
+    if (h->staging) return LBM_OK;
+    CK(cudaMalloc((void**)&h->staging, sizeof(double) * Q * (size_t)h->n), "staging allocation");
+    return LBM_OK;
+}
+
+int check_handle(const lbm_lattice* h)
+{
+    if (!h) return fail(LBM_ERR_INVALID, "null lattice handle");
+    CK(cudaSetDevice(h->desc.device), "cudaSetDevice");
+    return LBM_OK;
+}
+
+// Advance one step; rho/u/partials receive the readback of the state
+// before the step (optional).
+int advance(lbm_lattice* h, void* rho, void* u, double* partials)
+{
+    const void* src = h->buf[h->cur];
+    void* dst = h->buf[h->cur ^ 1];
+    cudaError_t e = launch(h, h->pre ? KERNEL_COLLIDE_LOCAL : KERNEL_STEP, src, dst, false, nullptr, rho, u, partials);
+    if (e != cudaSuccess) return cuda_fail(e, "step kernel launch");
+    h->cur ^= 1;
+    h->pre = false;
+    h->steps += 1;
+    return LBM_OK;
+}
+
+// Copy a device readback pair (C = double or float) into host f64 arrays.
+int readback_to_host(lbm_lattice* h, const void* drho, const void* du, double* rho, double* u)
+{
+    const size_t n = (size_t)h->n;
+    if (h->storage == LBM_STORAGE_F64) {
+        if (rho) CK(cudaMemcpyAsync(rho, drho, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream), "rho copy");
+        if (u) CK(cudaMemcpyAsync(u, du, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream), "u copy");
+        CK(cudaStreamSynchronize(h->stream), "readback sync");
+        return LBM_OK;
+    }
+    std::vector<float> tmp(4 * n);
+    CK(cudaMemcpyAsync(tmp.data(), drho, sizeof(float) * n, cudaMemcpyDeviceToHost, h->stream), "rho copy");
+    CK(cudaMemcpyAsync(tmp.data() + n, du, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, h->stream), "u copy");
+    CK(cudaStreamSynchronize(h->stream), "readback sync");
+    if (rho)
+        for (size_t i = 0; i < n; ++i) rho[i] = (double)tmp[i];
+    if (u)
+        for (size_t i = 0; i < 3 * n; ++i) u[i] = (double)tmp[n + i];
+    return LBM_OK;
+}
+
+int observe_rho_u(lbm_lattice* h, void* drho, void* du)
+{
+    cudaError_t e = launch(h, KERNEL_OBSERVE, h->buf[h->cur], nullptr, !h->pre, nullptr, drho, du, nullptr);
+    if (e != cudaSuccess) return cuda_fail(e, "observe kernel launch");
+    return LBM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_version(void) { return 10000; }
+
+const char* lbm_last_error(void) { return g_err.c_str(); }
+
+int lbm_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+int lbm_desc_init(lbm_desc* d)
+{
+    if (!d) return fail(LBM_ERR_INVALID, "null descriptor");
+    std::memset(d, 0, sizeof(*d));
+    d->nx = d->ny = d->nz = 1;
+    d->storage = LBM_STORAGE_F64;
+    d->periodic = LBM_PERIODIC_X | LBM_PERIODIC_Y | LBM_PERIODIC_Z;
+    d->force_mode = LBM_FORCE_NONE;
+    d->tau = 1.0;
+    d->inflow_rho = 1.0;
+    return LBM_OK;
+}
+
+int lbm_create(const lbm_desc* desc, lbm_lattice** out)
+{
+    if (!desc || !out) return fail(LBM_ERR_INVALID, "null argument to lbm_create");
+    *out = nullptr;
+    if (!dims_ok(desc->nx, desc->ny, desc->nz))
+        return fail(LBM_ERR_INVALID, "invalid lattice dimensions %d x %d x %d (need >= 1 and < 2^31 cells)",
+                    desc->nx, desc->ny, desc->nz);
+    if (storage_bytes(desc->storage) == 0) return fail(LBM_ERR_INVALID, "unknown storage %d", desc->storage);
+    if (desc->force_mode < LBM_FORCE_NONE || desc->force_mode > LBM_FORCE_DRAG)
+        return fail(LBM_ERR_INVALID, "unknown force mode %d", desc->force_mode);
+    if (!(desc->tau > 0.5)) return fail(LBM_ERR_INVALID, "tau must be > 0.5 (got %g)", desc->tau);
+    if (desc->periodic < 0 || desc->periodic > 7) return fail(LBM_ERR_INVALID, "periodic mask must be 0..7");
+    if (desc->block_size != 0 && (desc->block_size % 32 != 0 || desc->block_size < 32 || desc->block_size > 512))
+        return fail(LBM_ERR_INVALID, "block_size must be 0 or a multiple of 32 in [32, 512]");
+    int ndev = lbm_device_count();
+    if (ndev == 0) return fail(LBM_ERR_NO_DEVICE, "no CUDA device available");
+    if (desc->device < 0 || desc->device >= ndev) return fail(LBM_ERR_INVALID, "device %d out of range", desc->device);
+    CK(cudaSetDevice(desc->device), "cudaSetDevice");
+
+    lbm_lattice* h = new lbm_lattice();
+    h->desc = *desc;
+    h->storage = desc->storage;
+    h->n = desc->nx * desc->ny * desc->nz;
+    h->elem = storage_bytes(desc->storage);
+    h->block = desc->block_size ? desc->block_size : 256;
+    auto cleanup = [&](int code) {
+        lbm_destroy(h);
+        return code;
+    };
+    cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "stream creation"));
+    h->own_stream = true;
+    const size_t pop_bytes = h->elem * Q * (size_t)h->n;
+    for (int b = 0; b < 2; ++b) {
+        e = cudaMalloc(&h->buf[b], pop_bytes);
+        if (e != cudaSuccess) return cleanup(cuda_fail(e, "population allocation"));
+    }
+    const size_t cbytes = h->storage == LBM_STORAGE_F64 ? sizeof(double) : sizeof(float);
+    e = cudaMalloc(&h->rho, cbytes * (size_t)h->n);
+    if (e == cudaSuccess) e = cudaMalloc(&h->u, cbytes * 3 * (size_t)h->n);
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "readback allocation"));
+    h->partial_blocks = grid_for(h->n, h->block);
+    e = cudaMalloc((void**)&h->partials, sizeof(double) * 5 * (size_t)h->partial_blocks);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&h->sums, sizeof(double) * 5);
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "reduction scratch allocation"));
+    rebuild_params(h);
+    // Rest state f = w_i (rho = 1, u = 0).
+    e = launch_feq_init(h->storage, h->P, nullptr, nullptr, h->buf[0], h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "initial state"));
+    h->cur = 0;
+    h->pre = true;
+    *out = h;
+    return LBM_OK;
+}
+
+int lbm_destroy(lbm_lattice* h)
+{
+    if (!h) return LBM_OK;
+    cudaSetDevice(h->desc.device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    void* ptrs[] = {h->buf[0], h->buf[1], h->flags, h->force, h->poro, h->rho, h->u, h->partials, h->sums, h->staging};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return LBM_OK;
+}
+
+int lbm_set_stream(lbm_lattice* h, void* stream)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->stream), "stream sync");
+    if (h->own_stream) CK(cudaStreamDestroy(h->stream), "stream destroy");
+    h->own_stream = false;
+    if (stream) {
+        h->stream = (cudaStream_t)stream;
+    } else {
+        CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream creation");
+        h->own_stream = true;
+    }
+    return LBM_OK;
+}
+
+int lbm_synchronize(lbm_lattice* h)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->stream), "stream sync");
+    return LBM_OK;
+}
+
+int lbm_set_populations(lbm_lattice* h, const double* f)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!f) return fail(LBM_ERR_INVALID, "null population array");
+    const size_t bytes = sizeof(double) * Q * (size_t)h->n;
+    if (h->storage == LBM_STORAGE_F64) {
+        CK(cudaMemcpyAsync(h->buf[h->cur], f, bytes, cudaMemcpyHostToDevice, h->stream), "population upload");
+    } else {
+        if ((rc = ensure_staging(h))) return rc;
+        CK(cudaMemcpyAsync(h->staging, f, bytes, cudaMemcpyHostToDevice, h->stream), "population upload");
+        CK(launch_store_f64(h->storage, h->P, h->staging, h->buf[h->cur], h->stream), "population store");
+    }
+    CK(cudaStreamSynchronize(h->stream), "population upload sync");
+    h->pre = true;
+    return LBM_OK;
+}
+
+int lbm_get_populations(lbm_lattice* h, double* f)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!f) return fail(LBM_ERR_INVALID, "null population array");
+    const size_t bytes = sizeof(double) * Q * (size_t)h->n;
+    if (h->pre && h->storage == LBM_STORAGE_F64) {
+        CK(cudaMemcpyAsync(f, h->buf[h->cur], bytes, cudaMemcpyDeviceToHost, h->stream), "population download");
+    } else {
+        if ((rc = ensure_staging(h))) return rc;
+        if (h->pre) {
+            CK(launch_load_f64(h->storage, h->P, h->buf[h->cur], h->staging, h->stream), "population load");
+        } else {
+            CK(launch(h, KERNEL_OBSERVE, h->buf[h->cur], nullptr, true, h->staging, nullptr, nullptr, nullptr),
+               "population rebuild");
+        }
+        CK(cudaMemcpyAsync(f, h->staging, bytes, cudaMemcpyDeviceToHost, h->stream), "population download");
+    }
+    CK(cudaStreamSynchronize(h->stream), "population download sync");
+    return LBM_OK;
+}
+
+int lbm_set_equilibrium(lbm_lattice* h, const double* rho, const double* u)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    double* drho = nullptr;
+    double* du = nullptr;
+    const size_t n = (size_t)h->n;
+    if (rho || u) {
+        if ((rc = ensure_staging(h))) return rc;
+        drho = rho ? h->staging : nullptr;
+        du = u ? h->staging + n : nullptr;
+        if (rho) CK(cudaMemcpyAsync(drho, rho, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream), "rho upload");
+        if (u) CK(cudaMemcpyAsync(du, u, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream), "u upload");
+    }
+    CK(launch_feq_init(h->storage, h->P, drho, du, h->buf[h->cur], h->stream), "equilibrium init");
+    CK(cudaStreamSynchronize(h->stream), "equilibrium sync");
+    h->pre = true;
+    return LBM_OK;
+}
+
+int lbm_set_flags(lbm_lattice* h, const uint8_t* flags)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!flags) {
+        h->has_flags = false;
+        rebuild_params(h);
+        return LBM_OK;
+    }
+    const size_t n = (size_t)h->n;
+    for (size_t i = 0; i < n; ++i)
+        if (flags[i] > LBM_CELL_OUTFLOW)
+            return fail(LBM_ERR_INVALID, "flag value %u at cell %zu is not a cell type (0..3)", flags[i], i);
+    // A state held as P_{n-1} was built under the old flags; rebuild f_n
+    // under them first so that the change applies from the next step on.
+    if (!h->pre) {
+        if ((rc = ensure_staging(h))) return rc;
+        CK(launch(h, KERNEL_OBSERVE, h->buf[h->cur], nullptr, true, h->staging, nullptr, nullptr, nullptr),
+           "state rebuild");
+    }
+    if (!h->flags) CK(cudaMalloc((void**)&h->flags, n), "flag allocation");
+    CK(cudaMemcpyAsync(h->flags, flags, n, cudaMemcpyHostToDevice, h->stream), "flag upload");
+    h->has_flags = true;
+    rebuild_params(h);
+    CK(launch_mark_near_solid(h->P, h->flags, h->stream), "flag marking");
+    if (!h->pre) {
+        CK(launch_store_f64(h->storage, h->P, h->staging, h->buf[h->cur], h->stream), "state store");
+        h->pre = true;
+    }
+    CK(cudaStreamSynchronize(h->stream), "flag sync");
+    return LBM_OK;
+}
+
+int lbm_set_force_field(lbm_lattice* h, const double* force)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!force) return fail(LBM_ERR_INVALID, "null force field");
+    if (h->desc.force_mode != LBM_FORCE_FIELD)
+        return fail(LBM_ERR_STATE, "lattice was not created with LBM_FORCE_FIELD");
+    const size_t cnt = 3 * (size_t)h->n;
+    if (h->storage == LBM_STORAGE_F64) {
+        if (!h->force) CK(cudaMalloc(&h->force, sizeof(double) * cnt), "force allocation");
+        CK(cudaMemcpyAsync(h->force, force, sizeof(double) * cnt, cudaMemcpyHostToDevice, h->stream), "force upload");
+        CK(cudaStreamSynchronize(h->stream), "force sync");
+    } else {
+        std::vector<float> tmp(cnt);
+        for (size_t i = 0; i < cnt; ++i) tmp[i] = (float)force[i];
+        if (!h->force) CK(cudaMalloc(&h->force, sizeof(float) * cnt), "force allocation");
+        CK(cudaMemcpyAsync(h->force, tmp.data(), sizeof(float) * cnt, cudaMemcpyHostToDevice, h->stream),
+           "force upload");
+        CK(cudaStreamSynchronize(h->stream), "force sync");
+    }
+    rebuild_params(h);
+    return LBM_OK;
+}
+
+int lbm_set_porosity(lbm_lattice* h, const float* alpha)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!alpha) return fail(LBM_ERR_INVALID, "null porosity field");
+    if (h->desc.force_mode != LBM_FORCE_DRAG)
+        return fail(LBM_ERR_STATE, "lattice was not created with LBM_FORCE_DRAG");
+    const size_t n = (size_t)h->n;
+    for (size_t i = 0; i < n; ++i)
+        if (!(alpha[i] >= 0.0f && alpha[i] <= 1.0f))
+            return fail(LBM_ERR_INVALID, "porosity at cell %zu is outside [0, 1]", i);
+    if (!h->poro) CK(cudaMalloc((void**)&h->poro, sizeof(float) * n), "porosity allocation");
+    CK(cudaMemcpyAsync(h->poro, alpha, sizeof(float) * n, cudaMemcpyHostToDevice, h->stream), "porosity upload");
+    CK(cudaStreamSynchronize(h->stream), "porosity sync");
+    rebuild_params(h);
+    return LBM_OK;
+}
+
+int lbm_set_tau(lbm_lattice* h, double tau)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!(tau > 0.5)) return fail(LBM_ERR_INVALID, "tau must be > 0.5 (got %g)", tau);
+    h->desc.tau = tau;
+    rebuild_params(h);
+    return LBM_OK;
+}
+
+int lbm_set_wall_velocity(lbm_lattice* h, int32_t face, const double* u3)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (face < 0 || face > 5 || !u3) return fail(LBM_ERR_INVALID, "bad face index or null velocity");
+    for (int a = 0; a < 3; ++a) h->desc.wall_velocity[face][a] = u3[a];
+    rebuild_params(h);
+    return LBM_OK;
+}
+
+int lbm_set_body_force(lbm_lattice* h, const double* f3)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!f3) return fail(LBM_ERR_INVALID, "null body force");
+    for (int a = 0; a < 3; ++a) h->desc.body_force[a] = f3[a];
+    rebuild_params(h);
+    return LBM_OK;
+}
+
+static int check_force_ready(lbm_lattice* h)
+{
+    if (h->desc.force_mode == LBM_FORCE_FIELD && !h->force)
+        return fail(LBM_ERR_STATE, "LBM_FORCE_FIELD lattice has no force field (lbm_set_force_field)");
+    if (h->desc.force_mode == LBM_FORCE_DRAG && !h->poro)
+        return fail(LBM_ERR_STATE, "LBM_FORCE_DRAG lattice has no porosity field (lbm_set_porosity)");
+    return LBM_OK;
+}
+
+int lbm_step(lbm_lattice* h, int32_t n_steps)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (n_steps < 0) return fail(LBM_ERR_INVALID, "negative step count");
+    if ((rc = check_force_ready(h))) return rc;
+    for (int32_t s = 0; s < n_steps; ++s)
+        if ((rc = advance(h, nullptr, nullptr, nullptr))) return rc;
+    return LBM_OK;
+}
+
+int64_t lbm_step_count(const lbm_lattice* h) { return h ? h->steps : -1; }
+
+int lbm_get_rho_u(lbm_lattice* h, double* rho, double* u)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if ((rc = check_force_ready(h))) return rc;
+    if ((rc = observe_rho_u(h, h->rho, h->u))) return rc;
+    return readback_to_host(h, h->rho, h->u, rho, u);
+}
+
+int lbm_run_capture(lbm_lattice* h, int32_t n_steps, int32_t every, double* rho_frames, double* u_frames)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (n_steps < 0 || every < 1) return fail(LBM_ERR_INVALID, "need n_steps >= 0 and every >= 1");
+    if (!rho_frames || !u_frames) return fail(LBM_ERR_INVALID, "null frame buffer");
+    if ((rc = check_force_ready(h))) return rc;
+    const size_t n = (size_t)h->n;
+    int frame = 0;
+    for (int32_t s = 0; s <= n_steps; ++s) {
+        const bool need = (s % every == 0) || (s == n_steps);
+        if (s < n_steps) {
+            // The step kernel reads back the state it advances from (step s).
+            if ((rc = advance(h, need ? h->rho : nullptr, need ? h->u : nullptr, nullptr))) return rc;
+        } else if (need) {
+            if ((rc = observe_rho_u(h, h->rho, h->u))) return rc;
+        }
+        if (need) {
+            rc = readback_to_host(h, h->rho, h->u, rho_frames + frame * n, u_frames + frame * 3 * n);
+            if (rc) return rc;
+            ++frame;
+        }
+    }
+    return LBM_OK;
+}
+
+int lbm_conservation(lbm_lattice* h, double* out4)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!out4) return fail(LBM_ERR_INVALID, "null output");
+    if ((rc = check_force_ready(h))) return rc;
+    cudaError_t e = launch(h, KERNEL_OBSERVE, h->buf[h->cur], nullptr, !h->pre, nullptr, nullptr, nullptr, h->partials);
+    if (e != cudaSuccess) return cuda_fail(e, "conservation kernel");
+    CK(launch_reduce_partials(h->partials, h->partial_blocks, h->sums, h->stream), "partial reduction");
+    double s[5];
+    CK(cudaMemcpyAsync(s, h->sums, sizeof(s), cudaMemcpyDeviceToHost, h->stream), "sum copy");
+    CK(cudaStreamSynchronize(h->stream), "sum sync");
+    // f32-arithmetic storages sum density deviations; add the cell count back.
+    out4[0] = h->storage == LBM_STORAGE_F64 ? s[0] : s[0] + s[4];
+    out4[1] = s[1];
+    out4[2] = s[2];
+    out4[3] = s[3];
+    return LBM_OK;
+}
+
+int lbm_check_health(lbm_lattice* h)
+{
+    double s[4];
+    int rc = lbm_conservation(h, s);
+    if (rc) return rc;
+    for (double v : s)
+        if (!(v == v) || v == 1.0 / 0.0 || v == -1.0 / 0.0)
+            return fail(LBM_ERR_NONFINITE, "non-finite density or momentum in the lattice");
+    return LBM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Stateless reference functions
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Workspace {
+    std::mutex mu;
+    int device = -1;
+    double* ptr = nullptr;
+    size_t cap = 0;  // doubles
+};
+Workspace g_ws;
+
+// Device scratch for the host-array functions: holds inputs and outputs.
+int workspace(size_t doubles, double** out)
+{
+    int dev = 0;
+    CK(cudaGetDevice(&dev), "cudaGetDevice");
+    if (g_ws.ptr && (g_ws.cap < doubles || g_ws.device != dev)) {
+        cudaFree(g_ws.ptr);
+        g_ws.ptr = nullptr;
+        g_ws.cap = 0;
+    }
+    if (!g_ws.ptr) {
+        CK(cudaMalloc((void**)&g_ws.ptr, sizeof(double) * doubles), "workspace allocation");
+        g_ws.cap = doubles;
+        g_ws.device = dev;
+    }
+    *out = g_ws.ptr;
+    return LBM_OK;
+}
+
+int ref_params(int nx, int ny, int nz, Params& P)
+{
+    if (!dims_ok(nx, ny, nz)) return fail(LBM_ERR_INVALID, "invalid lattice dimensions %d x %d x %d", nx, ny, nz);
+    if (lbm_device_count() == 0) return fail(LBM_ERR_NO_DEVICE, "no CUDA device available");
+    init_geometry(P, nx, ny, nz);
+    return LBM_OK;
+}
+
+int finish(cudaError_t e, const char* what, cudaStream_t s)
+{
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    CK(cudaStreamSynchronize(s), what);
+    return LBM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_release_workspace(void)
+{
+    std::lock_guard<std::mutex> lk(g_ws.mu);
+    if (g_ws.ptr) cudaFree(g_ws.ptr);
+    g_ws.ptr = nullptr;
+    g_ws.cap = 0;
+    return LBM_OK;
+}
+
+int lbm_feq_field_dev(const double* rho, const double* u, double* feq, int32_t nx, int32_t ny, int32_t nz,
+                      void* stream)
+{
+    Params P;
+    int rc = ref_params(nx, ny, nz, P);
+    if (rc) return rc;
+    if (!rho || !u || !feq) return fail(LBM_ERR_INVALID, "null pointer");
+    return finish(ref_feq_field(P, rho, u, feq, (cudaStream_t)stream), "feq_field", (cudaStream_t)stream);
+}
+
+int lbm_density_field_dev(const double* f, double* rho, int32_t nx, int32_t ny, int32_t nz, void* stream)
+{
+    Params P;
+    int rc = ref_params(nx, ny, nz, P);
+    if (rc) return rc;
+    if (!f || !rho) return fail(LBM_ERR_INVALID, "null pointer");
+    return finish(ref_density(P, f, rho, (cudaStream_t)stream), "density_field", (cudaStream_t)stream);
+}
+
+int lbm_momentum_field_dev(const double* f, double* mom, int32_t nx, int32_t ny, int32_t nz, void* stream)
+{
+    Params P;
+    int rc = ref_params(nx, ny, nz, P);
+    if (rc) return rc;
+    if (!f || !mom) return fail(LBM_ERR_INVALID, "null pointer");
+    return finish(ref_momentum(P, f, mom, (cudaStream_t)stream), "momentum_field", (cudaStream_t)stream);
+}
+
+int lbm_macroscopic_velocity_dev(const double* f, const double* force, double* u, int32_t nx, int32_t ny,
+                                 int32_t nz, void* stream)
+{
+    Params P;
+    int rc = ref_params(nx, ny, nz, P);
+    if (rc) return rc;
+    if (!f || !u) return fail(LBM_ERR_INVALID, "null pointer");
+    return finish(ref_macro_velocity(P, f, force, u, (cudaStream_t)stream), "macroscopic_velocity",
+                  (cudaStream_t)stream);
+}
+
+int lbm_stream_dev(const double* f_post, double* f_out, int32_t nx, int32_t ny, int32_t nz, void* stream)
+{
+    Params P;
+    int rc = ref_params(nx, ny, nz, P);
+    if (rc) return rc;
+    if (!f_post || !f_out || f_post == f_out) return fail(LBM_ERR_INVALID, "null or aliased pointer");
+    return finish(ref_stream(P, f_post, f_out, (cudaStream_t)stream), "stream", (cudaStream_t)stream);
+}
+
+int lbm_bgk_step_dev(const double* f, double* f_out, double tau, const double* force, int32_t nx, int32_t ny,
+                     int32_t nz, void* stream)
+{
+    Params P;
+    int rc = ref_params(nx, ny, nz, P);
+    if (rc) return rc;
+    if (!f || !f_out || f == f_out) return fail(LBM_ERR_INVALID, "null or aliased pointer");
+    P.tau = tau;
+    return finish(ref_bgk_step(P, f, force, f_out, (cudaStream_t)stream), "bgk_step", (cudaStream_t)stream);
+}
+
+int lbm_bounce_back_y_walls_dev(const double* f, double* f_out, int32_t nx, int32_t ny, int32_t nz,
+                                const double* top, const double* bottom, void* stream)
+{
+    Params P;
+    int rc = ref_params(nx, ny, nz, P);
+    if (rc) return rc;
+    if (!f || !f_out || f == f_out) return fail(LBM_ERR_INVALID, "null or aliased pointer");
+    for (int a = 0; a < 3; ++a) {
+        P.wall_u[FACE_YP][a] = top ? top[a] : 0.0;
+        P.wall_u[FACE_YM][a] = bottom ? bottom[a] : 0.0;
+    }
+    return finish(ref_bounce_y(P, f, f_out, (cudaStream_t)stream), "apply_bounce_back_y_walls", (cudaStream_t)stream);
+}
+
+// Host-array variants: copy in, run on the default stream, copy out.
+#define HOST_PROLOGUE(ndoubles)                              \
+    std::lock_guard<std::mutex> lk(g_ws.mu);                 \
+    if (lbm_device_count() == 0) return fail(LBM_ERR_NO_DEVICE, "no CUDA device available"); \
+    if (!dims_ok(nx, ny, nz)) return fail(LBM_ERR_INVALID, "invalid lattice dimensions"); \
+    const size_t n = (size_t)nx * ny * nz;                   \
+    double* ws = nullptr;                                    \
+    int rc_ = workspace((ndoubles), &ws);                    \
+    if (rc_) return rc_;
+
+static int up(double* dst, const double* src, size_t cnt)
+{
+    CK(cudaMemcpy(dst, src, sizeof(double) * cnt, cudaMemcpyHostToDevice), "host-to-device copy");
+    return LBM_OK;
+}
+static int down(double* dst, const double* src, size_t cnt)
+{
+    CK(cudaMemcpy(dst, src, sizeof(double) * cnt, cudaMemcpyDeviceToHost), "device-to-host copy");
+    return LBM_OK;
+}
+
+int lbm_feq_field(const double* rho, const double* u, double* feq, int32_t nx, int32_t ny, int32_t nz)
+{
+    if (!rho || !u || !feq) return fail(LBM_ERR_INVALID, "null pointer");
+    HOST_PROLOGUE(23 * n)
+    int rc;
+    if ((rc = up(ws, rho, n)) || (rc = up(ws + n, u, 3 * n))) return rc;
+    if ((rc = lbm_feq_field_dev(ws, ws + n, ws + 4 * n, nx, ny, nz, nullptr))) return rc;
+    return down(feq, ws + 4 * n, 19 * n);
+}
+
+int lbm_density_field(const double* f, double* rho, int32_t nx, int32_t ny, int32_t nz)
+{
+    if (!f || !rho) return fail(LBM_ERR_INVALID, "null pointer");
+    HOST_PROLOGUE(20 * n)
+    int rc;
+    if ((rc = up(ws, f, 19 * n))) return rc;
+    if ((rc = lbm_density_field_dev(ws, ws + 19 * n, nx, ny, nz, nullptr))) return rc;
+    return down(rho, ws + 19 * n, n);
+}
+
+int lbm_momentum_field(const double* f, double* mom, int32_t nx, int32_t ny, int32_t nz)
+{
+    if (!f || !mom) return fail(LBM_ERR_INVALID, "null pointer");
+    HOST_PROLOGUE(22 * n)
+    int rc;
+    if ((rc = up(ws, f, 19 * n))) return rc;
+    if ((rc = lbm_momentum_field_dev(ws, ws + 19 * n, nx, ny, nz, nullptr))) return rc;
+    return down(mom, ws + 19 * n, 3 * n);
+}
+
+int lbm_macroscopic_velocity(const double* f, const double* force, double* u, int32_t nx, int32_t ny, int32_t nz)
+{
+    if (!f || !u) return fail(LBM_ERR_INVALID, "null pointer");
+    HOST_PROLOGUE(25 * n)
+    int rc;
+    if ((rc = up(ws, f, 19 * n))) return rc;
+    if (force && (rc = up(ws + 22 * n, force, 3 * n))) return rc;
+    if ((rc = lbm_macroscopic_velocity_dev(ws, force ? ws + 22 * n : nullptr, ws + 19 * n, nx, ny, nz, nullptr)))
+        return rc;
+    return down(u, ws + 19 * n, 3 * n);
+}
+
+int lbm_stream(const double* f_post, double* f_out, int32_t nx, int32_t ny, int32_t nz)
+{
+    if (!f_post || !f_out) return fail(LBM_ERR_INVALID, "null pointer");
+    HOST_PROLOGUE(38 * n)
+    int rc;
+    if ((rc = up(ws, f_post, 19 * n))) return rc;
+    if ((rc = lbm_stream_dev(ws, ws + 19 * n, nx, ny, nz, nullptr))) return rc;
+    return down(f_out, ws + 19 * n, 19 * n);
+}
+
+int lbm_bgk_step(const double* f, double* f_out, double tau, const double* force, int32_t nx, int32_t ny,
+                 int32_t nz)
+{
+    if (!f || !f_out) return fail(LBM_ERR_INVALID, "null pointer");
+    HOST_PROLOGUE(41 * n)
+    int rc;
+    if ((rc = up(ws, f, 19 * n))) return rc;
+    if (force && (rc = up(ws + 38 * n, force, 3 * n))) return rc;
+    if ((rc = lbm_bgk_step_dev(ws, ws + 19 * n, tau, force ? ws + 38 * n : nullptr, nx, ny, nz, nullptr)))
+        return rc;
+    return down(f_out, ws + 19 * n, 19 * n);
+}
+
+int lbm_bounce_back_y_walls(const double* f, double* f_out, int32_t nx, int32_t ny, int32_t nz, const double* top,
+                            const double* bottom)
+{
+    if (!f || !f_out) return fail(LBM_ERR_INVALID, "null pointer");
+    HOST_PROLOGUE(38 * n)
+    int rc;
+    if ((rc = up(ws, f, 19 * n))) return rc;
+    if ((rc = lbm_bounce_back_y_walls_dev(ws, ws + 19 * n, nx, ny, nz, top, bottom, nullptr))) return rc;
+    return down(f_out, ws + 19 * n, 19 * n);
+}
+
+}  // extern "C"

@@ -1,0 +1,561 @@
+// lbm_device.cuh -- device-side building blocks of the D3Q19 engine.
+//
+// Lattice: the reference's lex D3Q19 order
+//   (packages/lattice-boltzmann-d3q19-stack-e/lattice_boltzmann_d3q19_stack_e/
+//    reference/constants.py:27-57, opposite map d3q19_warp.py:61-64).
+// Layout in HBM: structure of arrays, direction-major, (19, nx, ny, nz) with z
+// contiguous; a cell index is (x*ny + y)*nz + z < 2^31.
+//
+// Two arithmetic modes share the gather / boundary code:
+//   ModeExact      f64 storage; every operation in the reference's order
+//                  (d3q19_warp.py:143-195, bgk.py:145-216).  Built with
+//                  --fmad=false so the result is bit-identical to the
+//                  reference on the same inputs.
+//   ModeFast<T>    f32 arithmetic on deviations h_i = f_i - w_i, storage T in
+//                  {float (holds f), __half (holds h), __nv_bfloat16 (holds h)}.
+#pragma once
+
+#include <cstdint>
+#include <type_traits>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+namespace lbm {
+
+constexpr int Q = 19;
+
+enum CellType : int { CELL_FLUID = 0, CELL_SOLID = 1, CELL_INFLOW = 2, CELL_OUTFLOW = 3 };
+// Internal flag bit: the cell has a solid cell among its 18 pull sources.
+constexpr int FLAG_NEAR_SOLID = 0x80;
+enum ForceMode : int { FORCE_NONE = 0, FORCE_UNIFORM = 1, FORCE_FIELD = 2, FORCE_DRAG = 3 };
+enum Face : int { FACE_XM = 0, FACE_XP = 1, FACE_YM = 2, FACE_YP = 3, FACE_ZM = 4, FACE_ZP = 5 };
+
+__host__ __device__ constexpr int cx(int d)
+{
+    return (d == 1 || d == 7 || d == 9 || d == 11 || d == 13) ? 1
+         : (d == 2 || d == 8 || d == 10 || d == 12 || d == 14) ? -1 : 0;
+}
+__host__ __device__ constexpr int cy(int d)
+{
+    return (d == 3 || d == 7 || d == 10 || d == 15 || d == 17) ? 1
+         : (d == 4 || d == 8 || d == 9 || d == 16 || d == 18) ? -1 : 0;
+}
+__host__ __device__ constexpr int cz(int d)
+{
+    return (d == 5 || d == 11 || d == 14 || d == 15 || d == 18) ? 1
+         : (d == 6 || d == 12 || d == 13 || d == 16 || d == 17) ? -1 : 0;
+}
+__host__ __device__ constexpr int opp(int d) { return d == 0 ? 0 : ((d & 1) ? d + 1 : d - 1); }
+// f32 lattice weights (the f64 ones travel in Params so that they are the
+// host-computed values 1.0/3.0, 1.0/18.0, 1.0/36.0).
+__host__ __device__ constexpr float wf(int d) { return d == 0 ? (1.0f / 3.0f) : (d < 7 ? (1.0f / 18.0f) : (1.0f / 36.0f)); }
+
+// Division by an invariant divisor with a multiply-high (Granlund & Montgomery
+// 1994, "Division by invariant integers using multiplication", round-up
+// method): q = (umulhi(n, m) + n) >> l, exact for 0 <= n < 2^31.
+struct FastDiv {
+    uint32_t d = 1, m = 1, l = 0;
+    __host__ void init(uint32_t div)
+    {
+        d = div;
+        l = 0;
+        while ((1ull << l) < div) ++l;
+        m = (uint32_t)((((1ull << 32) * ((1ull << l) - div)) / div) + 1);
+    }
+    __host__ __device__ __forceinline__ uint32_t div(uint32_t n) const
+    {
+#ifdef __CUDA_ARCH__
+        uint32_t t = __umulhi(n, m);
+#else
+        uint32_t t = (uint32_t)(((uint64_t)n * m) >> 32);
+#endif
+        return (t + n) >> l;
+    }
+};
+
+// Everything a step kernel needs to know about one lattice; passed by value.
+struct Params {
+    int nx, ny, nz, n, nynz;
+    FastDiv div_nz, div_ny;
+    int periodic;      // bit 0 x, 1 y, 2 z
+    int has_flags;
+    int wall_sum_pairwise; // nx * nz == 1 (see ModeExact::rho_wall)
+    const uint8_t* flags;
+    const void* force; // (3, n): double for ModeExact, float for ModeFast
+    const float* porosity;
+    // f64 values (ModeExact), all host-computed with the reference's expressions
+    double tau, cs2, inv_cs2, inv_cs4, inv_two_cs4, inv_two_cs2;
+    double w[Q];
+    double wall_u[6][3];
+    double body_force[3];
+    double drag_k;
+    double inflow_f[Q];
+    // f32 values (ModeFast)
+    float omega, pref;  // 1/tau, 1 - 0.5/tau
+    float wall_uf[6][3];
+    float body_force_f[3];
+    float drag_kf;
+    float inflow_h[Q];  // feq(inflow) - w
+};
+
+// np.maximum(rho, 1e-30): NaN propagates.
+__device__ __forceinline__ double rho_safe(double r) { return r != r ? r : (r > 1e-30 ? r : 1e-30); }
+__device__ __forceinline__ float rho_safe(float r) { return r != r ? r : (r > 1e-30f ? r : 1e-30f); }
+
+// ---------------------------------------------------------------------------
+// Storage loads / stores
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float ld_dev(const float* p, int d) { return __ldg(p) - wf(d); }
+__device__ __forceinline__ float ld_dev(const __half* p, int) { return __half2float(__ldg(p)); }
+__device__ __forceinline__ float ld_dev(const __nv_bfloat16* p, int) { return __bfloat162float(__ldg(p)); }
+__device__ __forceinline__ void st_dev(float* p, int d, float h) { *p = h + wf(d); }
+__device__ __forceinline__ void st_dev(__half* p, int, float h) { *p = __float2half_rn(h); }
+__device__ __forceinline__ void st_dev(__nv_bfloat16* p, int, float h) { *p = __float2bfloat16_rn(h); }
+// f64 value -> storage, rounding as the oracle's store_round does.
+__device__ __forceinline__ void st_f64(double* p, int, double v, const Params&) { *p = v; }
+__device__ __forceinline__ void st_f64(float* p, int, double v, const Params&) { *p = (float)v; }
+__device__ __forceinline__ void st_f64(__half* p, int d, double v, const Params& P)
+{
+    *p = __float2half_rn((float)(v - P.w[d]));
+}
+__device__ __forceinline__ void st_f64(__nv_bfloat16* p, int d, double v, const Params& P)
+{
+    *p = __float2bfloat16_rn((float)(v - P.w[d]));
+}
+// storage -> f64 value
+__device__ __forceinline__ double ld_f64(const double* p, int, const Params&) { return *p; }
+__device__ __forceinline__ double ld_f64(const float* p, int, const Params&) { return (double)*p; }
+__device__ __forceinline__ double ld_f64(const __half* p, int d, const Params& P)
+{
+    return P.w[d] + (double)__half2float(*p);
+}
+__device__ __forceinline__ double ld_f64(const __nv_bfloat16* p, int d, const Params& P)
+{
+    return P.w[d] + (double)__bfloat162float(*p);
+}
+
+// ---------------------------------------------------------------------------
+// Force at a cell (given the post-stream momentum for the drag model)
+// ---------------------------------------------------------------------------
+template <int FM>
+__device__ __forceinline__ void force_exact(const Params& P, int cell, double mx, double my, double mz,
+                                            double& Fx, double& Fy, double& Fz)
+{
+    if (FM == FORCE_UNIFORM) {
+        Fx = P.body_force[0]; Fy = P.body_force[1]; Fz = P.body_force[2];
+    } else if (FM == FORCE_FIELD) {
+        const double* F = (const double*)P.force;
+        Fx = F[cell]; Fy = F[P.n + cell]; Fz = F[2 * P.n + cell];
+    } else if (FM == FORCE_DRAG) {
+        double ka = P.drag_k * (double)P.porosity[cell];
+        double beta = ka / (1.0 + 0.5 * ka);
+        Fx = P.body_force[0] - beta * mx;
+        Fy = P.body_force[1] - beta * my;
+        Fz = P.body_force[2] - beta * mz;
+    } else {
+        Fx = Fy = Fz = 0.0;
+    }
+}
+
+template <int FM>
+__device__ __forceinline__ void force_fast(const Params& P, int cell, float mx, float my, float mz,
+                                           float& Fx, float& Fy, float& Fz)
+{
+    if (FM == FORCE_UNIFORM) {
+        Fx = P.body_force_f[0]; Fy = P.body_force_f[1]; Fz = P.body_force_f[2];
+    } else if (FM == FORCE_FIELD) {
+        const float* F = (const float*)P.force;
+        Fx = __ldg(F + cell); Fy = __ldg(F + P.n + cell); Fz = __ldg(F + 2 * P.n + cell);
+    } else if (FM == FORCE_DRAG) {
+        float ka = P.drag_kf * __ldg(P.porosity + cell);
+        float beta = ka / (1.0f + 0.5f * ka);
+        Fx = P.body_force_f[0] - beta * mx;
+        Fy = P.body_force_f[1] - beta * my;
+        Fz = P.body_force_f[2] - beta * mz;
+    } else {
+        Fx = Fy = Fz = 0.0f;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// ModeExact: f64, reference operation order
+// ---------------------------------------------------------------------------
+struct ModeExact {
+    using T = double;
+    using C = double;
+
+    static __device__ __forceinline__ C load(const T* p, int) { return __ldg(p); }
+    static __device__ __forceinline__ void store(T* p, int, C v) { *p = v; }
+    static __device__ __forceinline__ C solid(const Params& P, int d) { return P.w[d]; }
+    static __device__ __forceinline__ C inflow(const Params& P, int d) { return P.inflow_f[d]; }
+    static __device__ __forceinline__ double to_f64(const Params&, int, C v) { return v; }
+
+    // sum_d f[d] of the raw (pre-bounce) gather, bgk.py:203 / :212.  NumPy
+    // reduces a wall row in lex order, except when the row is a single cell
+    // (nx * nz == 1): then it runs its 8-accumulator pairwise summation.
+    static __device__ __forceinline__ C rho_wall(const Params& P, const C* f)
+    {
+        if (!P.wall_sum_pairwise) {
+            double r = 0.0;
+#pragma unroll
+            for (int d = 0; d < Q; ++d) r = r + f[d];
+            return r;
+        }
+        double a[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a[j] = f[j] + f[8 + j];
+        double r = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+#pragma unroll
+        for (int d = 16; d < Q; ++d) r = r + f[d];
+        return r;
+    }
+    // -2 w_i rho_w (c_i . u_w) / c_s^2 in the order of bgk.py:200-205.
+    static __device__ __forceinline__ C inject(const Params& P, int face, int d, C rho_w)
+    {
+        const double* uw = P.wall_u[face];
+        double ci_dot_uw = (double)cx(d) * uw[0] + (double)cy(d) * uw[1] + (double)cz(d) * uw[2];
+        return -2.0 * P.w[d] * rho_w * ci_dot_uw / P.cs2;
+    }
+
+    // _k_collide_guo (d3q19_warp.py:156-195); FORCE_NONE follows the NumPy
+    // force-free path of bgk.py:72-85 (no Guo term, u = m / rho_safe).
+    template <int FM>
+    static __device__ __forceinline__ void collide(const Params& P, int cell, C* f)
+    {
+        double r = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+#pragma unroll
+        for (int d = 0; d < Q; ++d) {
+            double fd = f[d];
+            r = r + fd;
+            mx = mx + (double)cx(d) * fd;
+            my = my + (double)cy(d) * fd;
+            mz = mz + (double)cz(d) * fd;
+        }
+        double rs = rho_safe(r);
+        double Fx, Fy, Fz;
+        force_exact<FM>(P, cell, mx, my, mz, Fx, Fy, Fz);
+        double ux, uy, uz;
+        if (FM == FORCE_NONE) {
+            ux = mx / rs; uy = my / rs; uz = mz / rs;
+        } else {
+            ux = mx / rs + 0.5 * Fx / rs;
+            uy = my / rs + 0.5 * Fy / rs;
+            uz = mz / rs + 0.5 * Fz / rs;
+        }
+        double u_sq = ux * ux + uy * uy + uz * uz;
+        double pref = 1.0 - 0.5 / P.tau;
+#pragma unroll
+        for (int d = 0; d < Q; ++d) {
+            double cd0 = (double)cx(d), cd1 = (double)cy(d), cd2 = (double)cz(d);
+            double cu = cd0 * ux + cd1 * uy + cd2 * uz;
+            double feq = P.w[d] * r * (1.0 + cu * P.inv_cs2 + cu * cu * P.inv_two_cs4 - u_sq * P.inv_two_cs2);
+            double fd = f[d];
+            double relaxed = fd - (fd - feq) / P.tau;
+            if (FM == FORCE_NONE) {
+                f[d] = relaxed;
+            } else {
+                double tx = (cd0 - ux) * P.inv_cs2 + cu * cd0 * P.inv_cs4;
+                double ty = (cd1 - uy) * P.inv_cs2 + cu * cd1 * P.inv_cs4;
+                double tz = (cd2 - uz) * P.inv_cs2 + cu * cd2 * P.inv_cs4;
+                double force_i = pref * P.w[d] * (tx * Fx + ty * Fy + tz * Fz);
+                f[d] = relaxed + force_i;
+            }
+        }
+    }
+
+    // density_field + macroscopic_velocity of one cell (d3q19_warp.py:111-140, :371-383).
+    template <int FM>
+    static __device__ __forceinline__ void readback(const Params& P, int cell, const C* f, C& rho, C* u)
+    {
+        double r = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+#pragma unroll
+        for (int d = 0; d < Q; ++d) {
+            double fd = f[d];
+            r = r + fd;
+            mx = mx + (double)cx(d) * fd;
+            my = my + (double)cy(d) * fd;
+            mz = mz + (double)cz(d) * fd;
+        }
+        double rs = rho_safe(r);
+        rho = r;
+        if (FM == FORCE_NONE) {
+            u[0] = mx / rs; u[1] = my / rs; u[2] = mz / rs;
+        } else {
+            double Fx, Fy, Fz;
+            force_exact<FM>(P, cell, mx, my, mz, Fx, Fy, Fz);
+            u[0] = (mx + 0.5 * Fx) / rs;
+            u[1] = (my + 0.5 * Fy) / rs;
+            u[2] = (mz + 0.5 * Fz) / rs;
+        }
+    }
+
+    // Mass contribution for the FP64 conservation sums.
+    static __device__ __forceinline__ void cons_terms(const C* f, double& mass, double& mx, double& my, double& mz)
+    {
+        double r = 0.0, a = 0.0, b = 0.0, c = 0.0;
+#pragma unroll
+        for (int d = 0; d < Q; ++d) {
+            r = r + f[d];
+            a = a + (double)cx(d) * f[d];
+            b = b + (double)cy(d) * f[d];
+            c = c + (double)cz(d) * f[d];
+        }
+        mass = r; mx = a; my = b; mz = c;
+    }
+    static constexpr bool mass_is_deviation = false;
+};
+
+// ---------------------------------------------------------------------------
+// ModeFast<T>: f32 arithmetic on deviations h = f - w
+// ---------------------------------------------------------------------------
+template <class TT>
+struct ModeFast {
+    using T = TT;
+    using C = float;
+
+    static __device__ __forceinline__ C load(const T* p, int d) { return ld_dev(p, d); }
+    static __device__ __forceinline__ void store(T* p, int d, C h) { st_dev(p, d, h); }
+    static __device__ __forceinline__ C solid(const Params&, int) { return 0.0f; }
+    static __device__ __forceinline__ C inflow(const Params& P, int d) { return P.inflow_h[d]; }
+    // The f64 population a stored deviation stands for: f32 storage holds
+    // f = h + w in f32; the 16-bit formats hold h, added to the f64 weight.
+    static __device__ __forceinline__ double to_f64(const Params& P, int d, C h)
+    {
+        if constexpr (std::is_same<TT, float>::value) return (double)(h + wf(d));
+        else return P.w[d] + (double)h;
+    }
+
+    static __device__ __forceinline__ C rho_wall(const Params&, const C* h)
+    {
+        float r = 0.0f;
+#pragma unroll
+        for (int d = 0; d < Q; ++d) r += h[d];
+        return 1.0f + r;
+    }
+    // In deviation form the reflected value keeps its weight (w_opp = w_i).
+    static __device__ __forceinline__ C inject(const Params& P, int face, int d, C rho_w)
+    {
+        const float* uw = P.wall_uf[face];
+        float ci_dot_uw = (float)cx(d) * uw[0] + (float)cy(d) * uw[1] + (float)cz(d) * uw[2];
+        return (-2.0f * 3.0f) * wf(d) * rho_w * ci_dot_uw;
+    }
+
+    // BGK + Guo in deviation form, opposite directions paired:
+    //   feq_i - w_i = w_i (rho_dev + rho (3 cu + 4.5 cu^2 - 1.5 u^2))
+    //   S_i = (1 - omega/2) w_i (3 (c_i - u).F + 9 (c_i.u)(c_i.F))
+    template <int FM>
+    static __device__ __forceinline__ void collide(const Params& P, int cell, C* h)
+    {
+        float rd = 0.0f, mx = 0.0f, my = 0.0f, mz = 0.0f;
+#pragma unroll
+        for (int d = 0; d < Q; ++d) {
+            rd += h[d];
+            if (cx(d) == 1) mx += h[d]; else if (cx(d) == -1) mx -= h[d];
+            if (cy(d) == 1) my += h[d]; else if (cy(d) == -1) my -= h[d];
+            if (cz(d) == 1) mz += h[d]; else if (cz(d) == -1) mz -= h[d];
+        }
+        float rho = 1.0f + rd;
+        float inv = 1.0f / rho_safe(rho);
+        float Fx, Fy, Fz;
+        force_fast<FM>(P, cell, mx, my, mz, Fx, Fy, Fz);
+        float ux, uy, uz;
+        if (FM == FORCE_NONE) {
+            ux = mx * inv; uy = my * inv; uz = mz * inv;
+        } else {
+            ux = (mx + 0.5f * Fx) * inv; uy = (my + 0.5f * Fy) * inv; uz = (mz + 0.5f * Fz) * inv;
+        }
+        const float om = P.omega;
+        const float usq15 = 1.5f * (ux * ux + uy * uy + uz * uz);
+        const float base = rd - rho * usq15; // rho_dev + rho(-1.5 u^2)
+        float uF3 = 0.0f, pref = 0.0f;
+        if (FM != FORCE_NONE) { uF3 = 3.0f * (ux * Fx + uy * Fy + uz * Fz); pref = P.pref; }
+        // rest direction
+        h[0] += om * (wf(0) * base - h[0]) - (FM != FORCE_NONE ? pref * wf(0) * uF3 : 0.0f);
+#pragma unroll
+        for (int d = 1; d < Q; d += 2) {
+            const int o = d + 1;
+            const float cu = (float)cx(d) * ux + (float)cy(d) * uy + (float)cz(d) * uz;
+            const float w = wf(d);
+            const float sym = w * (base + rho * 4.5f * cu * cu);
+            const float asym = w * rho * 3.0f * cu;
+            float hd = h[d] + om * (sym + asym - h[d]);
+            float ho = h[o] + om * (sym - asym - h[o]);
+            if (FM != FORCE_NONE) {
+                const float cF = (float)cx(d) * Fx + (float)cy(d) * Fy + (float)cz(d) * Fz;
+                const float s_sym = pref * w * (9.0f * cu * cF - uF3);
+                const float s_asym = pref * w * 3.0f * cF;
+                hd += s_sym + s_asym;
+                ho += s_sym - s_asym;
+            }
+            h[d] = hd;
+            h[o] = ho;
+        }
+    }
+
+    template <int FM>
+    static __device__ __forceinline__ void readback(const Params& P, int cell, const C* h, C& rho, C* u)
+    {
+        float rd = 0.0f, mx = 0.0f, my = 0.0f, mz = 0.0f;
+#pragma unroll
+        for (int d = 0; d < Q; ++d) {
+            rd += h[d];
+            if (cx(d) == 1) mx += h[d]; else if (cx(d) == -1) mx -= h[d];
+            if (cy(d) == 1) my += h[d]; else if (cy(d) == -1) my -= h[d];
+            if (cz(d) == 1) mz += h[d]; else if (cz(d) == -1) mz -= h[d];
+        }
+        float r = 1.0f + rd;
+        float rs = rho_safe(r);
+        rho = r;
+        if (FM == FORCE_NONE) {
+            u[0] = mx / rs; u[1] = my / rs; u[2] = mz / rs;
+        } else {
+            float Fx, Fy, Fz;
+            force_fast<FM>(P, cell, mx, my, mz, Fx, Fy, Fz);
+            u[0] = (mx + 0.5f * Fx) / rs;
+            u[1] = (my + 0.5f * Fy) / rs;
+            u[2] = (mz + 0.5f * Fz) / rs;
+        }
+    }
+
+    static __device__ __forceinline__ void cons_terms(const C* h, double& mass_dev, double& mx, double& my, double& mz)
+    {
+        float rd = 0.0f, a = 0.0f, b = 0.0f, c = 0.0f;
+#pragma unroll
+        for (int d = 0; d < Q; ++d) {
+            rd += h[d];
+            if (cx(d) == 1) a += h[d]; else if (cx(d) == -1) a -= h[d];
+            if (cy(d) == 1) b += h[d]; else if (cy(d) == -1) b -= h[d];
+            if (cz(d) == 1) c += h[d]; else if (cz(d) == -1) c -= h[d];
+        }
+        mass_dev = (double)rd; mx = (double)a; my = (double)b; mz = (double)c;
+    }
+    static constexpr bool mass_is_deviation = true;
+};
+
+// ---------------------------------------------------------------------------
+// Gather (pull streaming) and boundary rules
+// ---------------------------------------------------------------------------
+struct Site {
+    int x, y, z;   // the cell itself
+    int type;      // its type
+    int gx, gidx;  // gather position (x-1 for outflow cells) and its index
+    int gflag;     // flag byte at the gather position (outflow treated as fluid)
+};
+
+__device__ __forceinline__ Site decode_site(const Params& P, int idx)
+{
+    Site s;
+    uint32_t xy = P.div_nz.div((uint32_t)idx);
+    s.z = idx - (int)xy * P.nz;
+    uint32_t x = P.div_ny.div(xy);
+    s.y = (int)xy - (int)x * P.ny;
+    s.x = (int)x;
+    int fl = P.has_flags ? (int)P.flags[idx] : 0;
+    s.type = fl & 3;
+    s.gx = s.x;
+    s.gidx = idx;
+    s.gflag = fl;
+    if (s.type == CELL_OUTFLOW) {
+        s.gx = s.x == 0 ? P.nx - 1 : s.x - 1;
+        s.gidx = idx + (s.gx - s.x) * P.nynz;
+        int g = (int)P.flags[s.gidx];
+        if ((g & 3) == CELL_OUTFLOW) g &= ~3;
+        s.gflag = g;
+    }
+    return s;
+}
+
+// Index of the pull source x - c_d with periodic wrap (d3q19_warp.py:209-211),
+// from the wrapped neighbour coordinates precomputed per cell.
+struct Nbr {
+    int X[3], Y[3], Z[3]; // [0]: coordinate - 1, [1]: coordinate, [2]: coordinate + 1 (scaled)
+    __device__ __forceinline__ int src(int d) const { return X[1 - cx(d)] + Y[1 - cy(d)] + Z[1 - cz(d)]; }
+};
+
+__device__ __forceinline__ Nbr make_nbr(const Params& P, int gx, int y, int z)
+{
+    Nbr b;
+    int xm = gx == 0 ? P.nx - 1 : gx - 1, xp = gx == P.nx - 1 ? 0 : gx + 1;
+    int ym = y == 0 ? P.ny - 1 : y - 1, yp = y == P.ny - 1 ? 0 : y + 1;
+    int zm = z == 0 ? P.nz - 1 : z - 1, zp = z == P.nz - 1 ? 0 : z + 1;
+    b.X[0] = xm * P.nynz; b.X[1] = gx * P.nynz; b.X[2] = xp * P.nynz;
+    b.Y[0] = ym * P.nz; b.Y[1] = y * P.nz; b.Y[2] = yp * P.nz;
+    b.Z[0] = zm; b.Z[1] = z; b.Z[2] = zp;
+    return b;
+}
+
+__device__ __forceinline__ bool on_walled_face(const Params& P, int gx, int y, int z)
+{
+    return (!(P.periodic & 1) && (gx == 0 || gx == P.nx - 1)) ||
+           (!(P.periodic & 2) && (y == 0 || y == P.ny - 1)) ||
+           (!(P.periodic & 4) && (z == 0 || z == P.nz - 1));
+}
+
+// Walled face crossed by the pull source of direction d, or -1.  Priority when
+// several are crossed (edges / corners): y+, y-, x-, x+, z-, z+.
+__device__ __forceinline__ int crossed_face(const Params& P, int d, int gx, int y, int z)
+{
+    const bool wx = !(P.periodic & 1), wy = !(P.periodic & 2), wz = !(P.periodic & 4);
+    if (wy && cy(d) == -1 && y == P.ny - 1) return FACE_YP;
+    if (wy && cy(d) == 1 && y == 0) return FACE_YM;
+    if (wx && cx(d) == 1 && gx == 0) return FACE_XM;
+    if (wx && cx(d) == -1 && gx == P.nx - 1) return FACE_XP;
+    if (wz && cz(d) == 1 && z == 0) return FACE_ZM;
+    if (wz && cz(d) == -1 && z == P.nz - 1) return FACE_ZP;
+    return -1;
+}
+
+// Replace the pulled values that a boundary rule overrides.  Replacement
+// values are re-loaded from memory (never read from f[], which may already
+// hold replaced entries), so every rule sees the raw gather as the reference
+// does (bgk.py:190-216 reads its input f, writes a copy).
+template <class M>
+__device__ __forceinline__ void boundary_fix(const Params& P, const typename M::T* __restrict__ src,
+                                          typename M::C* f, const Nbr& nb, int gx, int y, int z, int gidx,
+                                          bool face_cell, bool near_solid)
+{
+    using C = typename M::C;
+    C rho_w = C(0);
+    if (face_cell) rho_w = M::rho_wall(P, f);
+#pragma unroll
+    for (int d = 1; d < Q; ++d) {
+        int face = face_cell ? crossed_face(P, d, gx, y, z) : -1;
+        if (face >= 0) {
+            const int o = opp(d);
+            C raw_o = M::load(src + (size_t)o * P.n + nb.src(o), o);
+            f[d] = raw_o + M::inject(P, face, d, rho_w);
+        } else if (near_solid) {
+            if ((P.flags[nb.src(d)] & 3) == CELL_SOLID) {
+                const int o = opp(d);
+                f[d] = M::load(src + (size_t)o * P.n + gidx, o);
+            }
+        }
+    }
+}
+
+// Post-stream (pre-collision) state of the cell described by s, pulled from
+// the stored post-collision array src.  Not called for solid cells.
+template <class M>
+__device__ __forceinline__ void pull_state(const Params& P, const typename M::T* __restrict__ src, const Site& s,
+                                           typename M::C* f)
+{
+    const int gtype = s.gflag & 3;
+    if (gtype == CELL_INFLOW) {
+#pragma unroll
+        for (int d = 0; d < Q; ++d) f[d] = M::inflow(P, d);
+        return;
+    }
+    if (gtype == CELL_SOLID) {
+#pragma unroll
+        for (int d = 0; d < Q; ++d) f[d] = M::solid(P, d);
+        return;
+    }
+    Nbr nb = make_nbr(P, s.gx, s.y, s.z);
+#pragma unroll
+    for (int d = 0; d < Q; ++d) f[d] = M::load(src + (size_t)d * P.n + nb.src(d), d);
+    const bool face_cell = on_walled_face(P, s.gx, s.y, s.z);
+    const bool near_solid = (s.gflag & FLAG_NEAR_SOLID) != 0;
+    if (face_cell || near_solid) boundary_fix<M>(P, src, f, nb, s.gx, s.y, s.z, s.gidx, face_cell, near_solid);
+}
+
+}  // namespace lbm

@@ -1,0 +1,52 @@
+// lbm_fast.cu -- f32-arithmetic step kernels for f32, binary16-shift and
+// bfloat16-shift storage (ModeFast).  Built with multiply-add contraction on.
+#include "lbm_kernels.cuh"
+#include "lbm_launch.h"
+
+namespace lbm {
+
+template <class T, int FM>
+static cudaError_t launch_fast_t(int kernel, const LaunchArgs& a)
+{
+    using M = ModeFast<T>;
+    Outputs<float> out{(float*)a.rho, (float*)a.u, a.partials};
+    const int grid = grid_for(a.P.n, a.block);
+    switch (kernel) {
+    case KERNEL_STEP:
+        k_step<M, FM><<<grid, a.block, 0, a.stream>>>(a.P, (const T*)a.src, (T*)a.dst, out);
+        break;
+    case KERNEL_COLLIDE_LOCAL:
+        k_collide_local<M, FM><<<grid, a.block, 0, a.stream>>>(a.P, (const T*)a.src, (T*)a.dst, out);
+        break;
+    case KERNEL_OBSERVE:
+        k_observe<M, FM><<<grid, a.block, 0, a.stream>>>(a.P, (const T*)a.src, a.post, a.f_out, out);
+        break;
+    default:
+        return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <class T>
+static cudaError_t launch_fast_fm(int kernel, int force_mode, const LaunchArgs& a)
+{
+    switch (force_mode) {
+    case FORCE_NONE: return launch_fast_t<T, FORCE_NONE>(kernel, a);
+    case FORCE_UNIFORM: return launch_fast_t<T, FORCE_UNIFORM>(kernel, a);
+    case FORCE_FIELD: return launch_fast_t<T, FORCE_FIELD>(kernel, a);
+    case FORCE_DRAG: return launch_fast_t<T, FORCE_DRAG>(kernel, a);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_fast(int storage, int kernel, int force_mode, const LaunchArgs& a)
+{
+    switch (storage) {
+    case STORAGE_F32: return launch_fast_fm<float>(kernel, force_mode, a);
+    case STORAGE_F16: return launch_fast_fm<__half>(kernel, force_mode, a);
+    case STORAGE_BF16: return launch_fast_fm<__nv_bfloat16>(kernel, force_mode, a);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace lbm

@@ -1,0 +1,50 @@
+// lbm_launch.h -- host-side launch entry points of the kernel translation
+// units (lbm_exact.cu: f64 reference-order arithmetic, built --fmad=false;
+// lbm_fast.cu: f32 arithmetic for f32 / f16 / bf16 storage).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "lbm_device.cuh"
+
+namespace lbm {
+
+enum StorageKind : int { STORAGE_F64 = 0, STORAGE_F32 = 1, STORAGE_F16 = 2, STORAGE_BF16 = 3 };
+enum KernelKind : int { KERNEL_STEP = 0, KERNEL_COLLIDE_LOCAL = 1, KERNEL_OBSERVE = 2 };
+
+struct LaunchArgs {
+    Params P;
+    const void* src;
+    void* dst;          // KERNEL_STEP / KERNEL_COLLIDE_LOCAL
+    bool post;          // KERNEL_OBSERVE: rebuild from a POST buffer
+    double* f_out;      // KERNEL_OBSERVE: optional f64 populations
+    void* rho;          // optional readback (double for f64 storage, float otherwise)
+    void* u;
+    double* partials;   // optional per-block conservation partials (grid x 5)
+    int block;
+    cudaStream_t stream;
+};
+
+inline int grid_for(long long work, int block) { return (int)((work + block - 1) / block); }
+
+// Stateful engine kernels.
+cudaError_t launch_exact(int kernel, int force_mode, const LaunchArgs& a);
+cudaError_t launch_fast(int storage, int kernel, int force_mode, const LaunchArgs& a);
+cudaError_t launch_store_f64(int storage, const Params& P, const double* f, void* dst, cudaStream_t s);
+cudaError_t launch_load_f64(int storage, const Params& P, const void* src, double* f, cudaStream_t s);
+cudaError_t launch_feq_init(int storage, const Params& P, const double* rho, const double* u, void* dst,
+                            cudaStream_t s);
+cudaError_t launch_mark_near_solid(const Params& P, uint8_t* flags, cudaStream_t s);
+cudaError_t launch_reduce_partials(const double* partials, int nblocks, double* out5, cudaStream_t s);
+
+// Stateless reference functions (f64, bit-exact), device pointers.
+cudaError_t ref_feq_field(const Params& P, const double* rho, const double* u, double* feq, cudaStream_t s);
+cudaError_t ref_density(const Params& P, const double* f, double* rho, cudaStream_t s);
+cudaError_t ref_momentum(const Params& P, const double* f, double* mom, cudaStream_t s);
+cudaError_t ref_macro_velocity(const Params& P, const double* f, const double* force, double* u,
+                               cudaStream_t s);
+cudaError_t ref_stream(const Params& P, const double* fin, double* fout, cudaStream_t s);
+cudaError_t ref_bgk_step(const Params& P, const double* f, const double* force, double* fout, cudaStream_t s);
+cudaError_t ref_bounce_y(const Params& P, const double* f, double* fout, cudaStream_t s);
+
+}  // namespace lbm

@@ -1,0 +1,218 @@
+"""Stateful lattice: populations resident on the GPU, stepped by fused kernels.
+
+Stands in for the state the reference's evolve loops carry between calls
+(``lattice_boltzmann_d3q19_stack_e/sim.py:119-190``: ``f = bgk_step(f, ...)``
+then ``f = apply_bounce_back_y_walls(f, ...)`` then ``density_field`` /
+``macroscopic_velocity``).  One ``step()`` is exactly one reference step; with
+f64 storage the result is bit-identical to the reference's.
+
+Beyond the reference (project semantics, pinned to the CPU oracle):
+* ``periodic``: any axis may be walled; a walled axis applies the
+  reference's y-wall rule on its two faces, each with its own velocity;
+* ``flags``: uint8 cell types -- fluid, solid (half-way bounce-back),
+  inflow (equilibrium at ``inflow_rho``/``inflow_u``), outflow
+  (zero-gradient copy of the x-1 neighbour);
+* ``force_mode``: none / uniform body force / per-cell field / porosity
+  drag F = body_force - beta(alpha) m with beta = k alpha / (1 + k alpha / 2);
+* ``storage``: f64 (reference order), f32, or 16-bit deviations from the
+  weights (f16 / bf16, "shift" storage) with f32 arithmetic.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+
+_FACE_ORDER = ("x-", "x+", "y-", "y+", "z-", "z+")
+
+
+def _periodic_mask(periodic) -> int:
+    if isinstance(periodic, int):
+        return periodic
+    px, py, pz = (bool(p) for p in periodic)
+    return (1 if px else 0) | (2 if py else 0) | (4 if pz else 0)
+
+
+class Lattice:
+    """A D3Q19 lattice on one GPU.  Arrays in and out are NumPy f64
+    (19, nx, ny, nz) / (nx, ny, nz) / (3, nx, ny, nz)."""
+
+    def __init__(
+        self,
+        shape,
+        tau,
+        *,
+        storage: str = "f64",
+        periodic=(True, True, True),
+        wall_velocity=None,
+        force_mode: str = "none",
+        body_force=(0.0, 0.0, 0.0),
+        drag_k: float = 0.0,
+        inflow_rho: float = 1.0,
+        inflow_u=(0.0, 0.0, 0.0),
+        device: int = 0,
+        block_size: int = 0,
+    ):
+        nx, ny, nz = (int(s) for s in shape)
+        if storage not in N.STORAGE:
+            raise ValueError(f"storage must be one of {sorted(N.STORAGE)}")
+        if force_mode not in N.FORCE:
+            raise ValueError(f"force_mode must be one of {sorted(N.FORCE)}")
+        self.shape = (nx, ny, nz)
+        self.n = nx * ny * nz
+        self.storage = storage
+        self.force_mode = force_mode
+        d = N.LbmDesc()
+        N.check(N.lib().lbm_desc_init(C.byref(d)))
+        d.nx, d.ny, d.nz = nx, ny, nz
+        d.storage = N.STORAGE[storage]
+        d.periodic = _periodic_mask(periodic)
+        d.force_mode = N.FORCE[force_mode]
+        d.tau = float(tau)
+        wu = self._wall_array(wall_velocity)
+        for k in range(18):
+            d.wall_velocity[k] = float(wu[k // 3, k % 3])
+        for k in range(3):
+            d.body_force[k] = float(body_force[k])
+            d.inflow_u[k] = float(inflow_u[k])
+        d.drag_k = float(drag_k)
+        d.inflow_rho = float(inflow_rho)
+        d.device = int(device)
+        d.block_size = int(block_size)
+        self.desc = d
+        h = C.c_void_p()
+        N.check(N.lib().lbm_create(C.byref(d), C.byref(h)))
+        self._h = h
+
+    @staticmethod
+    def _wall_array(wall_velocity) -> np.ndarray:
+        wu = np.zeros((6, 3))
+        if wall_velocity is None:
+            return wu
+        if isinstance(wall_velocity, dict):
+            for face, v in wall_velocity.items():
+                wu[N.FACES[face] if isinstance(face, str) else int(face)] = v
+            return wu
+        return N.f64(wall_velocity).reshape(6, 3)
+
+    # -- lifetime -----------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            N.lib().lbm_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    # -- state --------------------------------------------------------------
+    def set_populations(self, f) -> None:
+        f = N.f64(f)
+        if f.shape != (19, *self.shape):
+            raise ValueError(f"f must have shape {(19, *self.shape)}; got {f.shape}")
+        N.check(N.lib().lbm_set_populations(self._h, N.ptr(f)))
+
+    def get_populations(self) -> np.ndarray:
+        out = np.empty((19, *self.shape))
+        N.check(N.lib().lbm_get_populations(self._h, N.ptr(out)))
+        return out
+
+    def set_equilibrium(self, rho=None, u=None) -> None:
+        """f = feq(rho, u) (reciprocal form of equilibrium.py:310-322).  rho: scalar
+        or (nx,ny,nz), default 1; u: 3-vector or (3,nx,ny,nz), default 0."""
+        r = None if rho is None else N.f64(np.broadcast_to(N.f64(rho), self.shape))
+        v = None
+        if u is not None:
+            ua = N.f64(u)
+            if ua.shape == (3,):
+                ua = ua.reshape(3, 1, 1, 1)
+            v = N.f64(np.broadcast_to(ua, (3, *self.shape)))
+        N.check(N.lib().lbm_set_equilibrium(self._h, N.ptr(r), N.ptr(v)))
+
+    def set_flags(self, flags) -> None:
+        if flags is None:
+            N.check(N.lib().lbm_set_flags(self._h, None))
+            return
+        fl = np.ascontiguousarray(flags, dtype=np.uint8)
+        if fl.shape != self.shape:
+            raise ValueError(f"flags must have shape {self.shape}; got {fl.shape}")
+        self._flags = fl
+        N.check(N.lib().lbm_set_flags(self._h, N.ptr(fl, C.POINTER(C.c_uint8))))
+
+    def set_force_field(self, force) -> None:
+        F = N.f64(force)
+        if F.shape != (3, *self.shape):
+            raise ValueError(f"force must have shape {(3, *self.shape)}; got {F.shape}")
+        N.check(N.lib().lbm_set_force_field(self._h, N.ptr(F)))
+
+    def set_porosity(self, alpha) -> None:
+        a = np.ascontiguousarray(alpha, dtype=np.float32)
+        if a.shape != self.shape:
+            raise ValueError(f"porosity must have shape {self.shape}; got {a.shape}")
+        N.check(N.lib().lbm_set_porosity(self._h, N.ptr(a, C.POINTER(C.c_float))))
+
+    def set_tau(self, tau: float) -> None:
+        N.check(N.lib().lbm_set_tau(self._h, float(tau)))
+
+    def set_wall_velocity(self, face, u3) -> None:
+        idx = N.FACES[face] if isinstance(face, str) else int(face)
+        N.check(N.lib().lbm_set_wall_velocity(self._h, idx, N.ptr(N.f64(u3))))
+
+    def set_body_force(self, f3) -> None:
+        N.check(N.lib().lbm_set_body_force(self._h, N.ptr(N.f64(f3))))
+
+    # -- stepping and readback -----------------------------------------------
+    def step(self, n_steps: int = 1) -> None:
+        N.check(N.lib().lbm_step(self._h, int(n_steps)))
+
+    @property
+    def step_count(self) -> int:
+        return int(N.lib().lbm_step_count(self._h))
+
+    def rho_u(self) -> tuple[np.ndarray, np.ndarray]:
+        rho = np.empty(self.shape)
+        u = np.empty((3, *self.shape))
+        N.check(N.lib().lbm_get_rho_u(self._h, N.ptr(rho), N.ptr(u)))
+        return rho, u
+
+    def run_capture(self, n_steps: int, every: int = 1) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """Advance n_steps, reading rho/u at step 0, every `every` steps and at
+        the end.  Returns (steps, rho_frames, u_frames)."""
+        steps = list(range(0, n_steps + 1, every))
+        if steps[-1] != n_steps:
+            steps.append(n_steps)
+        rho = np.empty((len(steps), *self.shape))
+        u = np.empty((len(steps), 3, *self.shape))
+        N.check(N.lib().lbm_run_capture(self._h, int(n_steps), int(every), N.ptr(rho), N.ptr(u)))
+        return np.array(steps), rho, u
+
+    def conservation(self) -> np.ndarray:
+        """FP64 {sum rho, sum m_x, sum m_y, sum m_z} over non-solid cells."""
+        out = np.empty(4)
+        N.check(N.lib().lbm_conservation(self._h, N.ptr(out)))
+        return out
+
+    def check_health(self) -> bool:
+        rc = N.lib().lbm_check_health(self._h)
+        if rc == N.LBM_ERR_NONFINITE:
+            return False
+        N.check(rc)
+        return True
+
+    def synchronize(self) -> None:
+        N.check(N.lib().lbm_synchronize(self._h))

@@ -1,0 +1,193 @@
+/*
+ * lbm_d3q19.h -- C ABI of the B200 D3Q19 BGK lattice-Boltzmann engine
+ * (liblbm_d3q19.so, built from bit-physics_b200/csrc).
+ *
+ * Conventions
+ *   - Every function returns int status: LBM_OK (0) or a negative LBM_ERR_*
+ *     code; lbm_last_error() gives the calling thread's last message.  No
+ *     function aborts the process.
+ *   - Population arrays are structure-of-arrays f64 (19, nx, ny, nz), C order
+ *     (x slowest, z fastest), direction index in the reference's lex D3Q19
+ *     order (0 rest; 1-6 +-x,+-y,+-z; 7-10 xy; 11-14 xz; 15-18 yz).
+ *     rho is (nx, ny, nz); u and force fields are (3, nx, ny, nz).
+ *   - Host pointers are borrowed for the duration of the call.  A handle owns
+ *     its device memory.  Handles are not thread-safe: one thread per handle.
+ *
+ * Reference interface replaced (Bit-Physics, package
+ * packages/lattice-boltzmann-d3q19-stack-e/lattice_boltzmann_d3q19_stack_e/):
+ * the Python surface re-exported by reference/__init__.py:12-68 and the
+ * evolve loops of sim.py:119-190.  Each declaration cites the function it
+ * stands in for.
+ */
+#ifndef LBM_D3Q19_H
+#define LBM_D3Q19_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define LBM_OK 0
+#define LBM_ERR_INVALID (-1)     /* bad argument (shape, pointer, tau <= 0.5, ...) */
+#define LBM_ERR_CUDA (-2)        /* CUDA runtime error (message in lbm_last_error) */
+#define LBM_ERR_NOMEM (-3)       /* device or host allocation failed */
+#define LBM_ERR_STATE (-4)       /* call not valid in the handle's current state */
+#define LBM_ERR_NONFINITE (-5)   /* health check found a non-finite density */
+#define LBM_ERR_UNSUPPORTED (-6) /* combination not implemented */
+#define LBM_ERR_NO_DEVICE (-7)   /* no CUDA device / driver */
+
+/* ---- storage formats of the population arrays on the device ------------ */
+#define LBM_STORAGE_F64 0        /* f64, reference operation order (bit-exact)   */
+#define LBM_STORAGE_F32 1        /* f32 populations, f32 arithmetic               */
+#define LBM_STORAGE_F16_SHIFT 2  /* binary16 (f_i - w_i), f32 arithmetic          */
+#define LBM_STORAGE_BF16_SHIFT 3 /* bfloat16 (f_i - w_i), f32 arithmetic          */
+
+/* ---- periodicity bits; a non-periodic axis has two walled faces -------- */
+#define LBM_PERIODIC_X 1
+#define LBM_PERIODIC_Y 2
+#define LBM_PERIODIC_Z 4
+
+/* ---- domain faces (index into lbm_desc.wall_velocity) ------------------ */
+#define LBM_FACE_XM 0
+#define LBM_FACE_XP 1
+#define LBM_FACE_YM 2 /* the reference's bottom wall, y = 0      */
+#define LBM_FACE_YP 3 /* the reference's top wall,    y = ny - 1 */
+#define LBM_FACE_ZM 4
+#define LBM_FACE_ZP 5
+
+/* ---- cell types of the flag grid (uint8, one per cell) ----------------- */
+#define LBM_CELL_FLUID 0
+#define LBM_CELL_SOLID 1   /* static obstacle, half-way bounce-back            */
+#define LBM_CELL_INFLOW 2  /* post-stream state := feq(inflow_rho, inflow_u)   */
+#define LBM_CELL_OUTFLOW 3 /* post-stream state := that of cell (x-1, y, z)    */
+
+/* ---- body-force models -------------------------------------------------- */
+#define LBM_FORCE_NONE 0    /* force-free collision (bgk.py:72-85 path)          */
+#define LBM_FORCE_UNIFORM 1 /* F = body_force in every cell (Guo forcing)        */
+#define LBM_FORCE_FIELD 2   /* F from a per-cell (3, n) field (lbm_set_force_field) */
+#define LBM_FORCE_DRAG 3    /* F = body_force - beta(alpha) m, porosity alpha    */
+
+typedef struct lbm_desc {
+    int32_t nx, ny, nz;
+    int32_t storage;     /* LBM_STORAGE_*                                    */
+    int32_t periodic;    /* LBM_PERIODIC_* bits; default all periodic        */
+    int32_t force_mode;  /* LBM_FORCE_*                                      */
+    double tau;          /* BGK relaxation time, > 0.5                       */
+    double wall_velocity[6][3]; /* per face, used where the axis is walled   */
+    double body_force[3];
+    double drag_k;       /* drag coefficient k for LBM_FORCE_DRAG            */
+    double inflow_rho;   /* inflow cell density (default 1)                  */
+    double inflow_u[3];  /* inflow cell velocity                             */
+    int32_t device;      /* CUDA device ordinal                              */
+    int32_t block_size;  /* threads per block for the step kernels; 0 = auto */
+} lbm_desc;
+
+typedef struct lbm_lattice lbm_lattice;
+
+/* Fill a descriptor with defaults: 1x1x1, f64, all periodic, tau 1, no force. */
+int lbm_desc_init(lbm_desc* desc);
+
+/* ---- stateful engine ----------------------------------------------------
+ * Replaces the evolve loop of sim.py:119-190: state stays resident on the
+ * GPU; each step is one fused pull-stream + boundary + collide kernel. */
+
+/* Create a lattice handle; populations start at the rest equilibrium w_i. */
+int lbm_create(const lbm_desc* desc, lbm_lattice** out);
+int lbm_destroy(lbm_lattice* h);
+/* Use a caller-owned cudaStream_t (NULL: the handle's own stream). */
+int lbm_set_stream(lbm_lattice* h, void* cuda_stream);
+int lbm_synchronize(lbm_lattice* h);
+
+/* State in / out: stands in for the f array that the reference's loop
+ * carries between bgk_step and apply_bounce_back_y_walls (sim.py:140-142). */
+int lbm_set_populations(lbm_lattice* h, const double* f);
+int lbm_get_populations(lbm_lattice* h, double* f);
+/* Set f = feq(rho, u) on the device; rho may be NULL (1) and u NULL (0).
+ * Stands in for feq_field + the initial state (sim.py:112-116). */
+int lbm_set_equilibrium(lbm_lattice* h, const double* rho, const double* u);
+
+/* Boundary and forcing inputs. */
+int lbm_set_flags(lbm_lattice* h, const uint8_t* flags);     /* NULL clears */
+int lbm_set_force_field(lbm_lattice* h, const double* force); /* (3, n)     */
+int lbm_set_porosity(lbm_lattice* h, const float* alpha);     /* (n), [0,1] */
+int lbm_set_tau(lbm_lattice* h, double tau);
+int lbm_set_wall_velocity(lbm_lattice* h, int32_t face, const double* u3);
+int lbm_set_body_force(lbm_lattice* h, const double* f3);
+
+/* Advance n_steps: bgk_step + apply_bounce_back_y_walls per step
+ * (d3q19_warp.py:321-368, :386-415), generalised to the flag grid. */
+int lbm_step(lbm_lattice* h, int32_t n_steps);
+int64_t lbm_step_count(const lbm_lattice* h);
+
+/* rho and u of the current state: density_field + macroscopic_velocity
+ * (d3q19_warp.py:283-292, :371-383).  Either pointer may be NULL. */
+int lbm_get_rho_u(lbm_lattice* h, double* rho, double* u);
+
+/* Run n_steps and read back rho/u every `every` steps, plus the start and
+ * final states (sim.py:140-153 with capture_interval = every).  Frame k
+ * holds step k*every (the last frame step n_steps).  rho_frames holds
+ * n_frames*n, u_frames n_frames*3n doubles, n_frames = n_steps/every + 1
+ * (+1 when every does not divide n_steps). */
+int lbm_run_capture(lbm_lattice* h, int32_t n_steps, int32_t every, double* rho_frames,
+                    double* u_frames);
+
+/* FP64 sums over non-solid cells of the current state:
+ * out = {sum rho, sum m_x, sum m_y, sum m_z}. */
+int lbm_conservation(lbm_lattice* h, double* out4);
+
+/* Stateful health check: LBM_ERR_NONFINITE if any density is non-finite
+ * (the check_health diagnostic of sim.py:89-96). */
+int lbm_check_health(lbm_lattice* h);
+
+/* ---- stateless functions on host arrays ---------------------------------
+ * Same inputs, outputs and arithmetic as the reference's pure functions
+ * (f64, bit-exact); data is copied to the GPU and back on every call. */
+int lbm_feq_field(const double* rho, const double* u, double* feq, int32_t nx, int32_t ny,
+                  int32_t nz);                                        /* d3q19_warp.py:253 */
+int lbm_density_field(const double* f, double* rho, int32_t nx, int32_t ny,
+                      int32_t nz);                                    /* d3q19_warp.py:283 */
+int lbm_momentum_field(const double* f, double* mom, int32_t nx, int32_t ny,
+                       int32_t nz);                                   /* d3q19_warp.py:295 */
+int lbm_macroscopic_velocity(const double* f, const double* force, double* u, int32_t nx,
+                             int32_t ny, int32_t nz);                 /* d3q19_warp.py:371 */
+int lbm_stream(const double* f_post, double* f_out, int32_t nx, int32_t ny,
+               int32_t nz);                                           /* d3q19_warp.py:308 */
+int lbm_bgk_step(const double* f, double* f_out, double tau, const double* force, int32_t nx,
+                 int32_t ny, int32_t nz);                             /* d3q19_warp.py:321 */
+int lbm_bounce_back_y_walls(const double* f, double* f_out, int32_t nx, int32_t ny, int32_t nz,
+                            const double* wall_velocity_top,
+                            const double* wall_velocity_bottom);      /* d3q19_warp.py:386 */
+
+/* ---- the same functions on device pointers (no copies; stream may be NULL) */
+int lbm_feq_field_dev(const double* rho, const double* u, double* feq, int32_t nx, int32_t ny,
+                      int32_t nz, void* stream);
+int lbm_density_field_dev(const double* f, double* rho, int32_t nx, int32_t ny, int32_t nz,
+                          void* stream);
+int lbm_momentum_field_dev(const double* f, double* mom, int32_t nx, int32_t ny, int32_t nz,
+                           void* stream);
+int lbm_macroscopic_velocity_dev(const double* f, const double* force, double* u, int32_t nx,
+                                 int32_t ny, int32_t nz, void* stream);
+int lbm_stream_dev(const double* f_post, double* f_out, int32_t nx, int32_t ny, int32_t nz,
+                   void* stream);
+int lbm_bgk_step_dev(const double* f, double* f_out, double tau, const double* force, int32_t nx,
+                     int32_t ny, int32_t nz, void* stream);
+int lbm_bounce_back_y_walls_dev(const double* f, double* f_out, int32_t nx, int32_t ny,
+                                int32_t nz, const double* wall_velocity_top,
+                                const double* wall_velocity_bottom, void* stream);
+
+/* ---- library ------------------------------------------------------------ */
+const char* lbm_last_error(void);
+int lbm_version(void);
+/* Number of visible CUDA devices (0 when there is no driver or device). */
+int lbm_device_count(void);
+/* Release the device workspace that the host-array functions cache. */
+int lbm_release_workspace(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LBM_D3Q19_H */

@@ -1,0 +1,86 @@
+"""GPU parity on the reference's canonical trajectories (Stack-E gate 14):
+every captured frame of rho and u bit-identical to the reference's, through
+the stateful engine and through the pure-function surface; the f32 /
+16-bit storages within stated tolerances of the same frames."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+from conftest import load_npz
+from helpers import same_bytes, sha
+
+from lattice_boltzmann_d3q19_b200 import reference as R
+from lattice_boltzmann_d3q19_b200 import sim
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "couette_32x16x3": (sim.couette_lattice, 32, 16, 500),
+    "poiseuille_64x32x3": (sim.poiseuille_lattice, 64, 32, 1000),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_engine_every_frame_bit_exact(name):
+    make, nx, ny, steps = CASES[name]
+    g = load_npz(f"{name}.npz")
+    with make(nx, ny, 3) as lat:
+        step_ids, rho, u = lat.run_capture(steps, 1)
+        f_final = lat.get_populations()
+    assert list(step_ids) == list(range(steps + 1))
+    assert [sha(r) for r in rho] == list(g["rho_sha256"])
+    assert [sha(v) for v in u] == list(g["u_sha256"])
+    assert same_bytes(f_final, g["f_final"])
+
+
+def test_pure_function_loop_couette_bit_exact():
+    """The reference's own loop shape (sim.py:175-182) on the GPU surface."""
+    g = load_npz("couette_32x16x3.npz")
+    f = R.feq_field(np.ones((32, 16, 3)), np.zeros((3, 32, 16, 3)))
+    for step in range(1, 501):
+        f = R.bgk_step(f, 0.7)
+        f = R.apply_bounce_back_y_walls(f, wall_velocity_top=(0.05, 0.0, 0.0))
+        if step in (1, 10, 100, 500):
+            assert same_bytes(R.density_field(f), g[f"rho_{step}"])
+            assert same_bytes(R.macroscopic_velocity(f), g[f"u_{step}"])
+    assert same_bytes(f, g["f_final"])
+
+
+def test_runner_capture_and_determinism(tmp_path):
+    """sim_runner_diagnostic twice: identical payloads (gate 10, IC-14)."""
+    a = sim.sim_runner_diagnostic(42, tmp_path / "a")
+    b = sim.sim_runner_diagnostic(42, tmp_path / "b")
+    za = np.load(a.with_suffix(".npz"))
+    zb = np.load(b.with_suffix(".npz"))
+    assert sorted(za.files) == sorted(zb.files)
+    assert "steps/50/state/u" in za.files and "steps/0/diagnostics/check_health" in za.files
+    for k in za.files:
+        assert za[k].tobytes() == zb[k].tobytes(), k
+    assert float(za["steps/50/diagnostics/check_health"]) == 0.0
+    assert float(za["steps/50/diagnostics/check_divergence_free"]) < 1.0
+
+
+# Tolerances for the f32-arithmetic storages against the reference's f64
+# frames (max abs over all cells and components; populations ~1, u <= 0.05).
+FAST_TOL = {
+    "f32": {"rho": 2e-6, "u": 2e-6},
+    "f16": {"rho": 2e-3, "u": 1e-3},
+    "bf16": {"rho": 2e-2, "u": 1e-2},
+}
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_fast_storage_within_tolerance(name, storage):
+    make, nx, ny, steps = CASES[name]
+    g = load_npz(f"{name}.npz")
+    with make(nx, ny, 3, storage=storage) as lat:
+        step_ids, rho, u = lat.run_capture(steps, 1)
+    for s in g["keep_steps"]:
+        s = int(s)
+        err_rho = float(np.max(np.abs(rho[s] - g[f"rho_{s}"])))
+        err_u = float(np.max(np.abs(u[s] - g[f"u_{s}"])))
+        print(f"{name} {storage} step {s}: max|d rho| = {err_rho:.3e}  max|d u| = {err_u:.3e}")
+        assert err_rho <= FAST_TOL[storage]["rho"]
+        assert err_u <= FAST_TOL[storage]["u"]

@@ -1,0 +1,224 @@
+"""GPU engine vs the CPU oracle on the extended boundary semantics.
+
+f64 storage: bit-exact (masks, flags, walls, inflow / outflow, drag, force
+fields, edge shapes).  f32 / f16 / bf16: within stated tolerances of the
+oracle run with the same storage rounding.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+from gpu_cases import cavity_case, channel_case, drag_case, pair, random_state
+from helpers import same_bytes
+
+import oracle as O
+from lattice_boltzmann_d3q19_b200 import Lattice, LbmError
+from lattice_boltzmann_d3q19_b200 import _native as N
+
+pytestmark = pytest.mark.gpu
+
+
+def _advance_and_compare(gpu, cpu, f0, steps, exact=True, tol=None):
+    gpu.set_populations(f0)
+    cpu.set_populations(f0)
+    # PRE-state readback first
+    rg, ug = gpu.rho_u()
+    rc, uc = cpu.rho_u()
+    for k, n in enumerate(steps):
+        gpu.step(n)
+        cpu.step(n)
+        fg, fc = gpu.get_populations(), cpu.get_populations()
+        rg, ug = gpu.rho_u()
+        rc, uc = cpu.rho_u()
+        if exact:
+            assert same_bytes(fg, fc), f"populations differ after chunk {k}: {np.max(np.abs(fg - fc)):.3e}"
+            assert same_bytes(rg, rc) and same_bytes(ug, uc)
+        else:
+            df, dr, du = (float(np.max(np.abs(a - b))) for a, b in ((fg, fc), (rg, rc), (ug, uc)))
+            print(f"chunk {k}: max|df|={df:.3e} max|drho|={dr:.3e} max|du|={du:.3e}")
+            assert df <= tol and dr <= tol * 4 and du <= tol * 4
+    assert gpu.step_count == sum(steps)
+
+
+@pytest.mark.parametrize(
+    "shape,periodic",
+    [
+        ((7, 6, 5), (True, True, True)),
+        ((9, 1, 4), (True, False, True)),
+        ((1, 5, 1), (True, False, True)),
+        ((1, 1, 1), (True, True, True)),
+        ((5, 4, 37), (False, True, False)),
+        ((31, 3, 2), (False, False, False)),
+    ],
+)
+def test_f64_walls_and_shapes_bit_exact(shape, periodic):
+    wall = {"x-": (0.01, 0.0, 0.02), "x+": (0.0, -0.02, 0.0), "y-": (0.0, 0.0, 0.01),
+            "y+": (0.05, 0.0, 0.0), "z-": (0.0, 0.03, 0.0), "z+": (-0.02, 0.0, 0.0)}
+    gpu, cpu = pair(shape, 0.63, periodic=periodic, wall_velocity=wall)
+    with gpu:
+        _advance_and_compare(gpu, cpu, random_state(shape, 11), [1, 1, 5, 13])
+
+
+def test_f64_cavity_bit_exact():
+    gpu, cpu = cavity_case()
+    with gpu:
+        _advance_and_compare(gpu, cpu, O.feq_field(np.ones(cpu.shape), np.zeros((3, *cpu.shape))), [1, 20, 40])
+
+
+def test_f64_sphere_channel_bit_exact():
+    (gpu, cpu), flags = channel_case()
+    assert (flags == 1).sum() > 0
+    f0 = O.feq_field(np.ones(cpu.shape), np.tile(np.array([0.04, 0, 0]).reshape(3, 1, 1, 1), (1, *cpu.shape)))
+    with gpu:
+        _advance_and_compare(gpu, cpu, f0, [1, 30, 30])
+        c_gpu, c_cpu = gpu.conservation(), cpu.conservation()
+        assert np.allclose(c_gpu, c_cpu, rtol=1e-12, atol=1e-12)
+
+
+def test_f64_drag_and_force_field_bit_exact():
+    gpu, cpu = drag_case()
+    with gpu:
+        _advance_and_compare(gpu, cpu, random_state(cpu.shape, 12, amp=0.02), [1, 25])
+    shape = (6, 5, 7)
+    F = 1e-4 * np.random.default_rng(3).standard_normal((3, *shape))
+    gpu, cpu = pair(shape, 0.8, periodic=(True, False, True), force_mode="field", force_field=F,
+                    wall_velocity={"y+": (0.02, 0.0, 0.0)})
+    with gpu:
+        _advance_and_compare(gpu, cpu, random_state(shape, 13), [1, 9])
+    gpu, cpu = pair(shape, 0.55, force_mode="uniform", body_force=(1e-5, -2e-6, 3e-6))
+    with gpu:
+        _advance_and_compare(gpu, cpu, random_state(shape, 14), [1, 9])
+
+
+def test_f64_block_sizes_agree():
+    shape = (13, 11, 7)
+    f0 = random_state(shape, 21)
+    outs = []
+    for bs in (32, 128, 512):
+        gpu, _ = pair(shape, 0.7, periodic=(False, True, True), block_size=bs)
+        with gpu:
+            gpu.set_populations(f0)
+            gpu.step(10)
+            outs.append(gpu.get_populations())
+    assert same_bytes(outs[0], outs[1]) and same_bytes(outs[0], outs[2])
+
+
+def test_set_flags_mid_run_matches_oracle():
+    shape = (10, 8, 6)
+    gpu, cpu = pair(shape, 0.7)
+    f0 = random_state(shape, 22)
+    flags = np.zeros(shape, dtype=np.uint8)
+    flags[4:6, 3:5, 2:4] = 1
+    with gpu:
+        gpu.set_populations(f0)
+        gpu.step(5)
+        cpu.set_populations(f0)
+        cpu.step(5)
+        gpu.set_flags(flags)
+        cpu2 = O.OracleLattice(shape, 0.7, flags=flags)
+        cpu2.set_populations(cpu.get_populations())
+        gpu.step(7)
+        cpu2.step(7)
+        assert same_bytes(gpu.get_populations(), cpu2.get_populations())
+
+
+def test_conservation_f64():
+    shape = (16, 12, 10)
+    gpu, cpu = pair(shape, 0.6)
+    f0 = random_state(shape, 23)
+    with gpu:
+        gpu.set_populations(f0)
+        cpu.set_populations(f0)
+        for _ in range(3):
+            a, b = gpu.conservation(), cpu.conservation()
+            assert np.allclose(a, b, rtol=1e-13, atol=1e-13)
+            gpu.step(4)
+            cpu.step(4)
+        assert gpu.check_health()
+
+
+FAST_TOL = {"f32": 2e-6, "f16": 2e-4, "bf16": 2e-3}
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
+def test_fast_storages_cavity(storage):
+    gpu, cpu = cavity_case(storage=storage)
+    with gpu:
+        _advance_and_compare(gpu, cpu, O.feq_field(np.ones(cpu.shape), np.zeros((3, *cpu.shape))), [1, 20, 40],
+                             exact=False, tol=FAST_TOL[storage])
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
+def test_fast_storages_channel_and_drag(storage):
+    (gpu, cpu), _ = channel_case(storage=storage)
+    f0 = O.feq_field(np.ones(cpu.shape), np.tile(np.array([0.04, 0, 0]).reshape(3, 1, 1, 1), (1, *cpu.shape)))
+    with gpu:
+        _advance_and_compare(gpu, cpu, f0, [1, 30], exact=False, tol=FAST_TOL[storage])
+        a, b = gpu.conservation(), cpu.conservation()
+        assert abs(a[0] - b[0]) <= 1e-4 * b[0]
+    gpu, cpu = drag_case(storage=storage)
+    with gpu:
+        _advance_and_compare(gpu, cpu, random_state(cpu.shape, 12, amp=0.02), [1, 25], exact=False,
+                             tol=FAST_TOL[storage])
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
+def test_fast_storage_run_to_run_identical(storage):
+    (gpu, _), _ = channel_case(storage=storage)
+    f0 = random_state(gpu.shape, 24, amp=0.01)
+    outs = []
+    with gpu:
+        for _ in range(2):
+            gpu.set_populations(f0)
+            gpu.step(17)
+            outs.append(gpu.get_populations())
+    assert same_bytes(outs[0], outs[1])
+
+
+def test_error_codes():
+    with Lattice((4, 4, 4), 0.7, force_mode="field") as lat:
+        with pytest.raises(LbmError) as e:
+            lat.step(1)
+        assert e.value.code == N.LBM_ERR_STATE
+    with Lattice((4, 4, 4), 0.7, force_mode="drag", drag_k=0.1) as lat:
+        with pytest.raises(LbmError) as e:
+            lat.set_porosity(np.full((4, 4, 4), 1.5, dtype=np.float32))
+        assert e.value.code == N.LBM_ERR_INVALID
+    with Lattice((4, 4, 4), 0.7) as lat:
+        bad = np.zeros((4, 4, 4), dtype=np.uint8)
+        bad[1, 1, 1] = 9
+        with pytest.raises(LbmError) as e:
+            lat.set_flags(bad)
+        assert e.value.code == N.LBM_ERR_INVALID
+        with pytest.raises(LbmError) as e:
+            lat.set_tau(0.5)
+        assert e.value.code == N.LBM_ERR_INVALID
+        with pytest.raises(LbmError):
+            lat.set_force_field(np.zeros((3, 4, 4, 4)))
+        assert N.lib().lbm_step(lat.handle, -1) == N.LBM_ERR_INVALID
+        assert N.lib().lbm_set_wall_velocity(lat.handle, 7, None) == N.LBM_ERR_INVALID
+
+
+def test_nonfinite_state_detected():
+    with Lattice((4, 4, 4), 0.7) as lat:
+        f = random_state((4, 4, 4), 25)
+        f[3, 1, 2, 3] = np.nan
+        lat.set_populations(f)
+        assert not lat.check_health()
+        lat.step(2)
+        assert not lat.check_health()
+
+
+def test_many_handles_and_stream():
+    lats = [Lattice((8, 8, 8), 0.6 + 0.01 * k, storage=("f64", "f32", "f16", "bf16")[k % 4]) for k in range(8)]
+    for lat in lats:
+        lat.set_equilibrium(1.0, (0.01, 0.0, 0.0))
+        lat.step(3)
+    for lat in lats:
+        rho, u = lat.rho_u()
+        assert np.allclose(u[0], 0.01, atol=1e-3)
+        lat.close()
+    assert N.lib().lbm_set_stream(C.c_void_p(), None) == N.LBM_ERR_INVALID
