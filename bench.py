@@ -1,0 +1,450 @@
+#!/usr/bin/env python
+"""D3Q19 lattice-Boltzmann throughput on one or more B200s.
+
+Workload (the headline configuration): channel flow past 40 random spheres,
+256 x 128 x 128 cells, tau = 0.56, uniform inflow u_x = 0.04 at x = 0,
+zero-gradient outflow at x = nx-1, periodic y/z, sphere radii U[4, 10],
+centres in the middle 60 % of x, seed 42, uint8 flag grid.  A step is one
+lattice update of every cell (one fused stream + boundary + collide kernel).
+The headline arm stores populations in f32; the same run is repeated with
+f16 / bf16 deviation storage and with the f64 build, and each storage's
+velocity error after the timed steps is stated against the f64 run.
+
+value     whole-job GLUPS (cells x steps / s, summed over ranks), populations
+          resident in HBM; CUDA events on the launching stream.
+e2e       the same metric through the public API with host buffers: upload of
+          the initial populations (pinned) and the flag grid, the steps with
+          per-step FP64 mass/momentum sums returned to the host, and the final
+          rho/u read back.
+roofline  algorithmic bytes per cell update (f32: 19*4*2 + 1 = 153 B) x cells
+          / average kernel time, against the measured HBM copy bandwidth.
+
+--impl reference times the reference's CPU algorithm (the f64 CPU oracle that
+reproduces it bit-exactly, all host threads) on a bounded sample.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from datetime import timedelta
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+for _p in (ROOT / "bit-physics_b200", ROOT / "oracle"):
+    if str(_p) not in sys.path:
+        sys.path.insert(0, str(_p))
+
+import numpy as np  # noqa: E402
+
+METRIC = "D3Q19 GLUPS + %HBM peak: FP32 vs FP16-store at stated err; adjoint/fwd time"
+SHAPE = (256, 128, 128)
+TAU = 0.56
+INFLOW_U = 0.04
+N_SPHERES = 40
+RADIUS = (4.0, 10.0)
+SEED = 42
+WORKLOAD = (
+    f"sphere-channel {SHAPE[0]}x{SHAPE[1]}x{SHAPE[2]}, {N_SPHERES} spheres r~U[4,10] seed {SEED}, "
+    f"tau {TAU}, inflow u_x {INFLOW_U}, zero-gradient outflow, periodic y/z"
+)
+# Algorithmic bytes per cell update: read + write 19 populations, 1 flag byte.
+BYTES_PER_CELL = {"f64": 19 * 8 * 2 + 1, "f32": 19 * 4 * 2 + 1, "f16": 19 * 2 * 2 + 1, "bf16": 19 * 2 * 2 + 1}
+FALLBACK_HBM_GBS = 6650.0
+PROFILE_SUMMARY = ROOT / "profiles" / "step_kernels_sphere_channel.md"
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+def peak_hbm() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_per_cell(storage: str):
+    """DRAM bytes per cell update of the step kernel from the committed ncu
+    summary (lines 'TRAFFIC <storage> <bytes_per_cell>'), or None."""
+    try:
+        for line in PROFILE_SUMMARY.read_text().splitlines():
+            parts = line.strip().strip("`").split()
+            if len(parts) == 3 and parts[0] == "TRAFFIC" and parts[1] == storage:
+                return float(parts[2])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi samples (100 ms) of the SM clock and throttle reasons; each
+    row carries nvidia-smi's own timestamp and the GPU's UUID."""
+
+    FIELDS = ("timestamp,uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.rows: list[list[str]] = []
+        self.proc = None
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100"]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    @staticmethod
+    def _epoch(ts: str):
+        from datetime import datetime
+
+        try:
+            return datetime.strptime(ts, "%Y/%m/%d %H:%M:%S.%f").timestamp()
+        except ValueError:
+            return None
+
+    def summary(self, t0: float, t1: float):
+        rows = [r for r in self.rows if len(r) == 9]
+        if self.uuid:
+            mine = [r for r in rows if r[1] == self.uuid]
+            rows = mine or rows
+        inside = [r for r in rows if (e := self._epoch(r[0])) is not None and t0 - 0.05 <= e <= t1 + 0.05]
+        window = "timed region"
+        if not inside:
+            inside = [r for r in rows if (e := self._epoch(r[0])) is not None and e <= t1 + 0.05][-3:]
+            window = "last samples before the end of the timed region"
+        if not inside:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "window": "none"}
+
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return None
+
+        reasons = sorted({self.REASONS[k] for r in inside for k in range(4) if r[5 + k].lower() == "active"})
+        sm = [v for r in inside if (v := num(r[2])) is not None]
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": num(inside[0][3]),
+            "power_w_max": max((num(r[4]) or 0.0) for r in inside),
+            "reasons": reasons,
+            "samples": len(inside),
+            "window": window,
+        }
+
+
+def channel_geometry():
+    from lattice_boltzmann_d3q19_b200 import geometry
+
+    flags, _ = geometry.sphere_channel(SHAPE, n_spheres=N_SPHERES, radius=RADIUS, seed=SEED)
+    return flags
+
+
+def make_lattice(storage: str, flags, device: int):
+    from lattice_boltzmann_d3q19_b200 import Lattice
+
+    lat = Lattice(SHAPE, TAU, storage=storage, inflow_u=(INFLOW_U, 0.0, 0.0), device=device)
+    lat.set_flags(flags)
+    lat.set_equilibrium(1.0, (INFLOW_U, 0.0, 0.0))
+    return lat
+
+
+# ---------------------------------------------------------------------------
+# reference arm / CPU baseline: the f64 CPU oracle on a bounded sample
+# ---------------------------------------------------------------------------
+def cpu_reference_rate(flags, budget_s: float, max_steps: int):
+    import oracle as O
+
+    threads = O.num_threads()
+    lat = O.OracleLattice(SHAPE, TAU, flags=flags, inflow_u=(INFLOW_U, 0.0, 0.0))
+    u0 = np.zeros((3, *SHAPE))
+    u0[0] = INFLOW_U
+    lat.set_populations(O.feq_field(np.ones(SHAPE), u0))
+    del u0
+    t = time.perf_counter()
+    lat.step(1)
+    first = time.perf_counter() - t
+    steps = int(max(1, min(max_steps, budget_s / max(first, 1e-6))))
+    t = time.perf_counter()
+    lat.step(steps)
+    dt = time.perf_counter() - t
+    n = SHAPE[0] * SHAPE[1] * SHAPE[2]
+    rate = n * steps / dt / 1e9
+    sample = (f"{steps} steps (after 1 warm-up step) of the {SHAPE[0]}x{SHAPE[1]}x{SHAPE[2]} sphere "
+              f"channel, f64 CPU oracle (reference operation order), OpenMP")
+    return rate, threads, steps, dt, sample
+
+
+def run_reference(args, rank: int):
+    if rank != 0:
+        return
+    flags = channel_geometry()
+    budget = float(os.environ.get("LBM_REF_BUDGET_S", "30"))
+    rate, cores, steps, dt, sample = cpu_reference_rate(flags, budget, max(1, args.steps))
+    line = {
+        "metric": METRIC,
+        "value": rate,
+        "unit": "GLUPS",
+        "impl": "reference",
+        "n_gpus": args.gpus,
+        "steps": steps,
+        "warmup": 1,
+        "ms_per_step": dt / steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "cells": int(np.prod(SHAPE)), "storage": "f64",
+                   "requested_steps": args.steps},
+        "cpu_baseline": {"value": rate, "unit": "GLUPS", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": rate, "unit": "GLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def timed_steps(lat, steps: int, stream, torch, dist_on: bool):
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    if dist_on:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    t0 = time.time()
+    start.record(stream)
+    lat.step(steps)
+    end.record(stream)
+    torch.cuda.synchronize()
+    t1 = time.time()
+    if dist_on:
+        torch.distributed.barrier()
+    return start.elapsed_time(end), t0, t1
+
+
+def run_ours(args, rank: int, world: int, local_rank: int):
+    import torch
+
+    dist_on = world > 1
+    if dist_on:
+        torch.distributed.init_process_group("nccl", timeout=timedelta(seconds=300))
+    torch.cuda.set_device(local_rank)
+    dev = local_rank
+    try:
+        uuid = str(torch.cuda.get_device_properties(dev).uuid)
+        dev_id = uuid if uuid.startswith("GPU-") else f"GPU-{uuid}"
+    except Exception:
+        dev_id = None
+    n = int(np.prod(SHAPE))
+    flags = channel_geometry()
+    stream = torch.cuda.Stream(device=dev)
+    sampler = ClockSampler(dev_id)
+    hbm, hbm_kind = peak_hbm()
+
+    def measure(storage: str, steps: int, warmup: int):
+        lat = make_lattice(storage, flags, dev)
+        lat.set_stream(stream.cuda_stream)
+        lat.step(warmup)
+        ms, t0, t1 = timed_steps(lat, steps, stream, torch, False)
+        if not lat.check_health():
+            raise RuntimeError(f"{storage}: non-finite state after {warmup + steps} steps")
+        rho, u = lat.rho_u()
+        lat.close()
+        return ms, t0, t1, rho, u
+
+    # headline arm (f32), timed across ranks
+    lat = make_lattice(args.storage, flags, dev)
+    lat.set_stream(stream.cuda_stream)
+    lat.step(args.warmup)
+    ms, t0, t1 = timed_steps(lat, args.steps, stream, torch, dist_on)
+    healthy = lat.check_health()
+    rho_h, u_h = lat.rho_u()
+    lat.close()
+    ms_max = ms
+    if dist_on:
+        t = torch.tensor([ms], device=f"cuda:{dev}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_max = float(t.item())
+    clocks = sampler.summary(t0, t1)
+    value = world * n * args.steps / (ms_max / 1e3) / 1e9
+    ms_per_step = ms_max / args.steps
+    bpc = BYTES_PER_CELL[args.storage]
+    achieved = n * bpc / (ms / args.steps / 1e3) / 1e9
+    tr = traffic_per_cell(args.storage)
+    roofline = {
+        "bound": "hbm",
+        "achieved": achieved,
+        "peak": hbm,
+        "peak_kind": hbm_kind,
+        "unit": "GB/s",
+        "frac": achieved / hbm,
+        "traffic": None if tr is None else tr * n,
+        "algorithmic_bytes_per_launch": n * bpc,
+        "kernel": f"k_step<{args.storage}> (fused pull-stream + boundary + BGK collide)",
+    }
+
+    # variants and precision (every rank runs them; no collectives inside)
+    variants, precision = {}, {}
+    if not args.skip_variants:
+        results = {args.storage: (ms, rho_h, u_h)}
+        for st in ("f16", "bf16", "f64"):
+            if st == args.storage:
+                continue
+            ms_v, _, _, rho_v, u_v = measure(st, args.steps, args.warmup)
+            results[st] = (ms_v, rho_v, u_v)
+        ref_rho, ref_u = results["f64"][1], results["f64"][2]
+        umax = float(np.max(np.sqrt((ref_u * ref_u).sum(axis=0))))
+        fluid = flags != 1
+        for st, (ms_v, rho_v, u_v) in results.items():
+            glups = n * args.steps / (ms_v / 1e3) / 1e9
+            ach = n * BYTES_PER_CELL[st] / (ms_v / args.steps / 1e3) / 1e9
+            variants[st] = {"glups": glups, "ms_per_step": ms_v / args.steps, "hbm_gbs": ach,
+                            "frac": ach / hbm, "bytes_per_cell": BYTES_PER_CELL[st]}
+            if st != "f64":
+                du = np.sqrt(((u_v - ref_u) ** 2).sum(axis=0))[fluid]
+                precision[st] = {
+                    "u_max_err_rel": float(du.max() / umax),
+                    "u_l2_err_rel": float(np.sqrt(np.mean(du**2)) / umax),
+                    "rho_max_err": float(np.max(np.abs(rho_v - ref_rho)[fluid])),
+                    "rho_l2_err": float(np.sqrt(np.mean((rho_v - ref_rho)[fluid] ** 2))),
+                }
+        precision["reference"] = f"f64 GPU build of the same kernel after {args.warmup + args.steps} steps; " \
+                                 f"u errors relative to max|u| = {umax:.4g}"
+        if "f16" in variants and args.storage in variants:
+            variants["f16_over_f32_glups"] = variants["f16"]["glups"] / variants[args.storage]["glups"]
+
+    # end to end through the public API with host buffers
+    e2e = None
+    if not args.skip_e2e:
+        import oracle as O
+
+        u0 = np.zeros((3, *SHAPE))
+        u0[0] = INFLOW_U
+        f0_pinned = torch.empty((19, *SHAPE), dtype=torch.float64, pin_memory=True).numpy()
+        f0_pinned[...] = O.feq_field(np.ones(SHAPE), u0)
+        del u0
+        from lattice_boltzmann_d3q19_b200 import Lattice
+
+        lat = Lattice(SHAPE, TAU, storage=args.storage, inflow_u=(INFLOW_U, 0.0, 0.0), device=dev)
+        lat.set_populations(f0_pinned)  # allocate staging outside the timed region
+        torch.cuda.synchronize()
+        if dist_on:
+            torch.distributed.barrier()
+        t = time.perf_counter()
+        lat.set_populations(f0_pinned)
+        lat.set_flags(flags)
+        sums = lat.step_monitor(args.steps)
+        rho_e, u_e = lat.rho_u()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t
+        lat.close()
+        if dist_on:
+            tt = torch.tensor([dt], device=f"cuda:{dev}", dtype=torch.float64)
+            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+            dt = float(tt.item())
+        out_bytes = 4 * n * (8 if args.storage == "f64" else 4)
+        e2e = {
+            "value": world * n * args.steps / dt / 1e9,
+            "unit": "GLUPS",
+            "h2d_bytes_per_step": (19 * 8 * n + n) / args.steps,
+            "d2h_bytes_per_step": (5 * 8 * args.steps + out_bytes) / args.steps,
+            "what": "set_populations (pinned f64) + set_flags + step_monitor (per-step FP64 mass/momentum "
+                    "sums to host) + rho_u readback, wall clock",
+            "mass_drift_rel": float((sums[-1, 0] - sums[0, 0]) / sums[0, 0]),
+        }
+    sampler.stop()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        rate, cores, steps, dt, sample = cpu_reference_rate(flags, float(os.environ.get("LBM_CPU_BUDGET_S", "15")),
+                                                            args.steps)
+        cpu = {"value": rate, "unit": "GLUPS", "cores": cores, "kind": "port", "sample": sample}
+
+    if dist_on:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "GLUPS",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": args.storage,
+        "data": "synthetic",
+        "config": {
+            "workload": WORKLOAD,
+            "cells": n,
+            "storage": args.storage,
+            "l2": f"inputs larger than L2: 2 x {19 * n * {'f64': 8, 'f32': 4}.get(args.storage, 2) / 1e6:.0f} MB "
+                  f"population buffers",
+            "parallelism": "replicas (one independent lattice per GPU)" if world > 1 else "single GPU",
+        },
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "clocks": clocks,
+        "gpu_launches": args.steps,
+        "healthy": healthy,
+        "variants": variants,
+        "precision": precision,
+        "adjoint_over_forward": None,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16", "f64"])
+    ap.add_argument("--skip-variants", action="store_true")
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        ap.error("--warmup must be >= 3")
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

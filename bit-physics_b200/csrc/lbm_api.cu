@@ -114,6 +114,8 @@ struct lbm_lattice {
     double* sums = nullptr;  // 5 doubles
     int partial_blocks = 0;
     double* staging = nullptr; // (19, n) f64, allocated on first use
+    double* monitor = nullptr; // (monitor_cap, 5) per-step sums of lbm_step_monitor
+    int monitor_cap = 0;
     int64_t steps = 0;
     int block = 256;
     Params P{};
@@ -322,7 +324,8 @@ int lbm_destroy(lbm_lattice* h)
     if (!h) return LBM_OK;
     cudaSetDevice(h->desc.device);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    void* ptrs[] = {h->buf[0], h->buf[1], h->flags, h->force, h->poro, h->rho, h->u, h->partials, h->sums, h->staging};
+    void* ptrs[] = {h->buf[0], h->buf[1], h->flags, h->force, h->poro, h->rho,
+                    h->u, h->partials, h->sums, h->staging, h->monitor};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -572,6 +575,40 @@ int lbm_run_capture(lbm_lattice* h, int32_t n_steps, int32_t every, double* rho_
             if (rc) return rc;
             ++frame;
         }
+    }
+    return LBM_OK;
+}
+
+int lbm_step_monitor(lbm_lattice* h, int32_t n_steps, double* sums)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (n_steps < 0) return fail(LBM_ERR_INVALID, "negative step count");
+    if (n_steps > 0 && !sums) return fail(LBM_ERR_INVALID, "null sums array");
+    if ((rc = check_force_ready(h))) return rc;
+    if (n_steps == 0) return LBM_OK;
+    if (h->monitor_cap < n_steps) {
+        if (h->monitor) CK(cudaFree(h->monitor), "monitor free");
+        h->monitor = nullptr;
+        h->monitor_cap = 0;
+        CK(cudaMalloc((void**)&h->monitor, sizeof(double) * 5 * (size_t)n_steps), "monitor allocation");
+        h->monitor_cap = n_steps;
+    }
+    for (int32_t s = 0; s < n_steps; ++s) {
+        if ((rc = advance(h, nullptr, nullptr, h->partials))) return rc;
+        CK(launch_reduce_partials(h->partials, h->partial_blocks, h->monitor + 5 * (size_t)s, h->stream),
+           "partial reduction");
+    }
+    std::vector<double> tmp(5 * (size_t)n_steps);
+    CK(cudaMemcpyAsync(tmp.data(), h->monitor, sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost, h->stream),
+       "monitor copy");
+    CK(cudaStreamSynchronize(h->stream), "monitor sync");
+    for (int32_t s = 0; s < n_steps; ++s) {
+        const double* v = tmp.data() + 5 * (size_t)s;
+        sums[4 * s + 0] = h->storage == LBM_STORAGE_F64 ? v[0] : v[0] + v[4];
+        sums[4 * s + 1] = v[1];
+        sums[4 * s + 2] = v[2];
+        sums[4 * s + 3] = v[3];
     }
     return LBM_OK;
 }

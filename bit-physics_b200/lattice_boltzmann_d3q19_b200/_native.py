@@ -82,6 +82,7 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "lbm_step_count": ([_h], C.c_int64),
     "lbm_get_rho_u": ([_h, _dp, _dp], C.c_int),
     "lbm_run_capture": ([_h, _i, _i, _dp, _dp], C.c_int),
+    "lbm_step_monitor": ([_h, _i, _dp], C.c_int),
     "lbm_conservation": ([_h, _dp], C.c_int),
     "lbm_check_health": ([_h], C.c_int),
     "lbm_feq_field": ([_dp, _dp, _dp, _i, _i, _i], C.c_int),

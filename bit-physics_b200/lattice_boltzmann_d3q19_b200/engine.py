@@ -201,6 +201,18 @@ class Lattice:
         N.check(N.lib().lbm_run_capture(self._h, int(n_steps), int(every), N.ptr(rho), N.ptr(u)))
         return np.array(steps), rho, u
 
+    def step_monitor(self, n_steps: int) -> np.ndarray:
+        """Advance n_steps; returns (n_steps, 4) FP64 {sum rho, sum m} of the
+        state each step advanced from, reduced on the GPU."""
+        out = np.empty((int(n_steps), 4))
+        N.check(N.lib().lbm_step_monitor(self._h, int(n_steps), N.ptr(out)))
+        return out
+
+    def set_stream(self, cuda_stream: int | None) -> None:
+        """Launch on a caller-owned cudaStream_t (an integer handle, e.g.
+        torch.cuda.Stream().cuda_stream); None restores the handle's own."""
+        N.check(N.lib().lbm_set_stream(self._h, C.c_void_p(cuda_stream) if cuda_stream else None))
+
     def conservation(self) -> np.ndarray:
         """FP64 {sum rho, sum m_x, sum m_y, sum m_z} over non-solid cells."""
         out = np.empty(4)

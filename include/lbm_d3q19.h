@@ -134,6 +134,13 @@ int lbm_get_rho_u(lbm_lattice* h, double* rho, double* u);
 int lbm_run_capture(lbm_lattice* h, int32_t n_steps, int32_t every, double* rho_frames,
                     double* u_frames);
 
+/* Advance n_steps and return, per step, the FP64 sums {sum rho, sum m_x,
+ * sum m_y, sum m_z} over non-solid cells of the state that step advanced
+ * from (sums: n_steps x 4 doubles).  The sums are reduced on the GPU inside
+ * the step kernels and copied to the host once, after the last step: the
+ * global mass / momentum drift check of a run (sim.py:89-96 health check). */
+int lbm_step_monitor(lbm_lattice* h, int32_t n_steps, double* sums);
+
 /* FP64 sums over non-solid cells of the current state:
  * out = {sum rho, sum m_x, sum m_y, sum m_z}. */
 int lbm_conservation(lbm_lattice* h, double* out4);

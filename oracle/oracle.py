@@ -289,17 +289,18 @@ class OracleLattice:
 
     def set_populations(self, f) -> None:
         self._a = store_round(self.storage, f).reshape((19, *self.shape))
+        self._spare = None
         self._pre = True
 
     def step(self, n_steps: int = 1) -> None:
         for _ in range(int(n_steps)):
-            b = np.empty_like(self._a)
+            b = self._spare if getattr(self, "_spare", None) is not None else np.empty_like(self._a)
             if self._pre:
                 lib().orc_engine_collide_local(self._L, _ptr(self._a), _ptr(b), None, None)
                 self._pre = False
             else:
                 lib().orc_engine_step(self._L, _ptr(self._a), _ptr(b), None, None)
-            self._a = b
+            self._spare, self._a = self._a, b
             self.step_count += 1
 
     def get_populations(self) -> np.ndarray:

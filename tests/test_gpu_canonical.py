@@ -63,10 +63,12 @@ def test_runner_capture_and_determinism(tmp_path):
 
 # Tolerances for the f32-arithmetic storages against the reference's f64
 # frames (max abs over all cells and components; populations ~1, u <= 0.05).
+# Measured on a B200 (Couette 500 / Poiseuille 1000 steps): f32 rho 3.6e-7,
+# u 2.2e-7; f16 rho 4.5e-5, u 8.2e-5; bf16 rho 4.4e-4, u 2.6e-3.
 FAST_TOL = {
-    "f32": {"rho": 2e-6, "u": 2e-6},
-    "f16": {"rho": 2e-3, "u": 1e-3},
-    "bf16": {"rho": 2e-2, "u": 1e-2},
+    "f32": {"rho": 1e-6, "u": 1e-6},
+    "f16": {"rho": 2e-4, "u": 4e-4},
+    "bf16": {"rho": 2e-3, "u": 1e-2},
 }
 
 
