@@ -105,6 +105,7 @@ struct lbm_lattice {
     int cur = 0;
     bool pre = true;
     uint8_t* flags = nullptr;
+    uint32_t* bbmask = nullptr; // (n) bounce-back masks, allocated with the flags
     bool has_flags = false;
     void* force = nullptr;   // (3, n) double (f64 storage) or float
     float* poro = nullptr;   // (n)
@@ -131,6 +132,7 @@ void rebuild_params(lbm_lattice* h)
     P.periodic = d.periodic & 7;
     P.has_flags = h->has_flags ? 1 : 0;
     P.flags = h->flags;
+    P.bbmask = h->bbmask;
     P.force = h->force;
     P.porosity = h->poro;
     P.tau = d.tau;
@@ -275,8 +277,8 @@ int lbm_create(const lbm_desc* desc, lbm_lattice** out)
         return fail(LBM_ERR_INVALID, "unknown force mode %d", desc->force_mode);
     if (!(desc->tau > 0.5)) return fail(LBM_ERR_INVALID, "tau must be > 0.5 (got %g)", desc->tau);
     if (desc->periodic < 0 || desc->periodic > 7) return fail(LBM_ERR_INVALID, "periodic mask must be 0..7");
-    if (desc->block_size != 0 && (desc->block_size % 32 != 0 || desc->block_size < 32 || desc->block_size > 512))
-        return fail(LBM_ERR_INVALID, "block_size must be 0 or a multiple of 32 in [32, 512]");
+    if (desc->block_size != 0 && (desc->block_size % 32 != 0 || desc->block_size < 32 || desc->block_size > 256))
+        return fail(LBM_ERR_INVALID, "block_size must be 0 or a multiple of 32 in [32, 256]");
     int ndev = lbm_device_count();
     if (ndev == 0) return fail(LBM_ERR_NO_DEVICE, "no CUDA device available");
     if (desc->device < 0 || desc->device >= ndev) return fail(LBM_ERR_INVALID, "device %d out of range", desc->device);
@@ -324,7 +326,7 @@ int lbm_destroy(lbm_lattice* h)
     if (!h) return LBM_OK;
     cudaSetDevice(h->desc.device);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    void* ptrs[] = {h->buf[0], h->buf[1], h->flags, h->force, h->poro, h->rho,
+    void* ptrs[] = {h->buf[0], h->buf[1], h->flags, h->bbmask, h->force, h->poro, h->rho,
                     h->u, h->partials, h->sums, h->staging, h->monitor};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -438,10 +440,11 @@ int lbm_set_flags(lbm_lattice* h, const uint8_t* flags)
            "state rebuild");
     }
     if (!h->flags) CK(cudaMalloc((void**)&h->flags, n), "flag allocation");
+    if (!h->bbmask) CK(cudaMalloc((void**)&h->bbmask, sizeof(uint32_t) * n), "mask allocation");
     CK(cudaMemcpyAsync(h->flags, flags, n, cudaMemcpyHostToDevice, h->stream), "flag upload");
     h->has_flags = true;
     rebuild_params(h);
-    CK(launch_mark_near_solid(h->P, h->flags, h->stream), "flag marking");
+    CK(launch_mark_near_solid(h->P, h->flags, h->bbmask, h->stream), "flag marking");
     if (!h->pre) {
         CK(launch_store_f64(h->storage, h->P, h->staging, h->buf[h->cur], h->stream), "state store");
         h->pre = true;

@@ -25,7 +25,8 @@ namespace lbm {
 constexpr int Q = 19;
 
 enum CellType : int { CELL_FLUID = 0, CELL_SOLID = 1, CELL_INFLOW = 2, CELL_OUTFLOW = 3 };
-// Internal flag bit: the cell has a solid cell among its 18 pull sources.
+// Internal flag bit: the cell has a solid cell among its 18 pull sources
+// (its bounce-back mask is nonzero).
 constexpr int FLAG_NEAR_SOLID = 0x80;
 enum ForceMode : int { FORCE_NONE = 0, FORCE_UNIFORM = 1, FORCE_FIELD = 2, FORCE_DRAG = 3 };
 enum Face : int { FACE_XM = 0, FACE_XP = 1, FACE_YM = 2, FACE_YP = 3, FACE_ZM = 4, FACE_ZP = 5 };
@@ -81,6 +82,7 @@ struct Params {
     int has_flags;
     int wall_sum_pairwise; // nx * nz == 1 (see ModeExact::rho_wall)
     const uint8_t* flags;
+    const uint32_t* bbmask; // (n): bit d set when the pull source of d is solid
     const void* force; // (3, n): double for ModeExact, float for ModeFast
     const float* porosity;
     // f64 values (ModeExact), all host-computed with the reference's expressions
@@ -435,41 +437,21 @@ struct ModeFast {
 // ---------------------------------------------------------------------------
 // Gather (pull streaming) and boundary rules
 // ---------------------------------------------------------------------------
-struct Site {
-    int x, y, z;   // the cell itself
-    int type;      // its type
-    int gx, gidx;  // gather position (x-1 for outflow cells) and its index
-    int gflag;     // flag byte at the gather position (outflow treated as fluid)
-};
 
-__device__ __forceinline__ Site decode_site(const Params& P, int idx)
-{
-    Site s;
-    uint32_t xy = P.div_nz.div((uint32_t)idx);
-    s.z = idx - (int)xy * P.nz;
-    uint32_t x = P.div_ny.div(xy);
-    s.y = (int)xy - (int)x * P.ny;
-    s.x = (int)x;
-    int fl = P.has_flags ? (int)P.flags[idx] : 0;
-    s.type = fl & 3;
-    s.gx = s.x;
-    s.gidx = idx;
-    s.gflag = fl;
-    if (s.type == CELL_OUTFLOW) {
-        s.gx = s.x == 0 ? P.nx - 1 : s.x - 1;
-        s.gidx = idx + (s.gx - s.x) * P.nynz;
-        int g = (int)P.flags[s.gidx];
-        if ((g & 3) == CELL_OUTFLOW) g &= ~3;
-        s.gflag = g;
-    }
-    return s;
-}
+// Per-direction base pointers of the source and destination population
+// buffers (kernel parameter; one multiply-add per access).
+template <class T>
+struct Streams {
+    const T* src[Q];
+    T* dst[Q];
+};
 
 // Index of the pull source x - c_d with periodic wrap (d3q19_warp.py:209-211),
 // from the wrapped neighbour coordinates precomputed per cell.
 struct Nbr {
     int X[3], Y[3], Z[3]; // [0]: coordinate - 1, [1]: coordinate, [2]: coordinate + 1 (scaled)
     __device__ __forceinline__ int src(int d) const { return X[1 - cx(d)] + Y[1 - cy(d)] + Z[1 - cz(d)]; }
+    __device__ __forceinline__ int dst(int d) const { return X[1 + cx(d)] + Y[1 + cy(d)] + Z[1 + cz(d)]; }
 };
 
 __device__ __forceinline__ Nbr make_nbr(const Params& P, int gx, int y, int z)
@@ -482,6 +464,15 @@ __device__ __forceinline__ Nbr make_nbr(const Params& P, int gx, int y, int z)
     b.Y[0] = ym * P.nz; b.Y[1] = y * P.nz; b.Y[2] = yp * P.nz;
     b.Z[0] = zm; b.Z[1] = z; b.Z[2] = zp;
     return b;
+}
+
+__device__ __forceinline__ void decode_xyz(const Params& P, int idx, int& x, int& y, int& z)
+{
+    const uint32_t xy = P.div_nz.div((uint32_t)idx);
+    z = idx - (int)xy * P.nz;
+    const uint32_t xx = P.div_ny.div(xy);
+    y = (int)xy - (int)xx * P.ny;
+    x = (int)xx;
 }
 
 __device__ __forceinline__ bool on_walled_face(const Params& P, int gx, int y, int z)
@@ -505,57 +496,85 @@ __device__ __forceinline__ int crossed_face(const Params& P, int d, int gx, int 
     return -1;
 }
 
+// Raw pull of all 19 directions at the position described by nb.
+template <class M>
+__device__ __forceinline__ void gather(const Streams<typename M::T>& S, const Nbr& nb, typename M::C* f)
+{
+#pragma unroll
+    for (int d = 0; d < Q; ++d) f[d] = M::load(S.src[d] + nb.src(d), d);
+}
+
 // Replace the pulled values that a boundary rule overrides.  Replacement
 // values are re-loaded from memory (never read from f[], which may already
 // hold replaced entries), so every rule sees the raw gather as the reference
-// does (bgk.py:190-216 reads its input f, writes a copy).
+// does (bgk.py:190-216 reads its input f and writes a copy).
+//   walled face crossed:  f[d] = raw[opp(d)] + injection(face, rho_w)
+//   solid source (mask):  f[d] = P[opp(d)] at the cell (half-way bounce-back)
 template <class M>
-__device__ __forceinline__ void boundary_fix(const Params& P, const typename M::T* __restrict__ src,
-                                          typename M::C* f, const Nbr& nb, int gx, int y, int z, int gidx,
-                                          bool face_cell, bool near_solid)
+__device__ __forceinline__ void boundary_fix(const Params& P, const Streams<typename M::T>& S, const Nbr& nb,
+                                             int gx, int y, int z, int gidx, bool face_cell, uint32_t bbmask,
+                                             typename M::C* f)
 {
     using C = typename M::C;
     C rho_w = C(0);
     if (face_cell) rho_w = M::rho_wall(P, f);
 #pragma unroll
     for (int d = 1; d < Q; ++d) {
-        int face = face_cell ? crossed_face(P, d, gx, y, z) : -1;
+        const int face = face_cell ? crossed_face(P, d, gx, y, z) : -1;
+        const int o = opp(d);
         if (face >= 0) {
-            const int o = opp(d);
-            C raw_o = M::load(src + (size_t)o * P.n + nb.src(o), o);
-            f[d] = raw_o + M::inject(P, face, d, rho_w);
-        } else if (near_solid) {
-            if ((P.flags[nb.src(d)] & 3) == CELL_SOLID) {
-                const int o = opp(d);
-                f[d] = M::load(src + (size_t)o * P.n + gidx, o);
-            }
+            f[d] = M::load(S.src[o] + nb.src(o), o) + M::inject(P, face, d, rho_w);
+        } else if ((bbmask >> d) & 1u) {
+            f[d] = M::load(S.src[o] + gidx, o);
         }
     }
 }
 
-// Post-stream (pre-collision) state of the cell described by s, pulled from
-// the stored post-collision array src.  Not called for solid cells.
+// Turn the speculative own-position gather f[] into the post-stream
+// (pre-collision) state of cell idx.  Returns false for a solid cell.
+//   inflow cell:   feq(inflow_rho, inflow_u)
+//   outflow cell:  the state of cell (x-1, y, z) (an outflow neighbour is
+//                  treated as fluid)
+//   fluid cell:    boundary_fix where it sits on a walled face or pulls from
+//                  a solid cell
 template <class M>
-__device__ __forceinline__ void pull_state(const Params& P, const typename M::T* __restrict__ src, const Site& s,
-                                           typename M::C* f)
+__device__ __forceinline__ bool resolve_state(const Params& P, const Streams<typename M::T>& S, int idx, int x,
+                                              int y, int z, int fl, const Nbr& nb, typename M::C* f)
 {
-    const int gtype = s.gflag & 3;
-    if (gtype == CELL_INFLOW) {
+    const bool face = on_walled_face(P, x, y, z);
+    if (fl == 0 && !face) return true;
+    const int type = fl & 3;
+    if (type == CELL_SOLID) return false;
+    if (type == CELL_INFLOW) {
 #pragma unroll
         for (int d = 0; d < Q; ++d) f[d] = M::inflow(P, d);
-        return;
+        return true;
     }
-    if (gtype == CELL_SOLID) {
+    if (type == CELL_OUTFLOW) {
+        const int gx = x == 0 ? P.nx - 1 : x - 1;
+        const int gidx = idx + (gx - x) * P.nynz;
+        int g = (int)P.flags[gidx];
+        if ((g & 3) == CELL_OUTFLOW) g &= ~3;
+        if ((g & 3) == CELL_INFLOW) {
 #pragma unroll
-        for (int d = 0; d < Q; ++d) f[d] = M::solid(P, d);
-        return;
+            for (int d = 0; d < Q; ++d) f[d] = M::inflow(P, d);
+            return true;
+        }
+        if ((g & 3) == CELL_SOLID) {
+#pragma unroll
+            for (int d = 0; d < Q; ++d) f[d] = M::solid(P, d);
+            return true;
+        }
+        const Nbr nb2 = make_nbr(P, gx, y, z);
+        gather<M>(S, nb2, f);
+        const bool face2 = on_walled_face(P, gx, y, z);
+        const uint32_t m = (g & FLAG_NEAR_SOLID) ? P.bbmask[gidx] : 0u;
+        if (face2 || m) boundary_fix<M>(P, S, nb2, gx, y, z, gidx, face2, m, f);
+        return true;
     }
-    Nbr nb = make_nbr(P, s.gx, s.y, s.z);
-#pragma unroll
-    for (int d = 0; d < Q; ++d) f[d] = M::load(src + (size_t)d * P.n + nb.src(d), d);
-    const bool face_cell = on_walled_face(P, s.gx, s.y, s.z);
-    const bool near_solid = (s.gflag & FLAG_NEAR_SOLID) != 0;
-    if (face_cell || near_solid) boundary_fix<M>(P, src, f, nb, s.gx, s.y, s.z, s.gidx, face_cell, near_solid);
+    const uint32_t m = (fl & FLAG_NEAR_SOLID) ? P.bbmask[idx] : 0u;
+    boundary_fix<M>(P, S, nb, x, y, z, idx, face, m, f);
+    return true;
 }
 
 }  // namespace lbm

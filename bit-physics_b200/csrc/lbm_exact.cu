@@ -15,24 +15,36 @@ namespace lbm {
 // ---------------------------------------------------------------------------
 // Stateful engine, f64 storage
 // ---------------------------------------------------------------------------
+template <class M, int FM, int OUT>
+static void launch_step_out(int kernel, const LaunchArgs& a, int grid)
+{
+    using T = typename M::T;
+    using C = typename M::C;
+    Outputs<C> out{(C*)a.rho, (C*)a.u, a.partials};
+    const Streams<T> S = make_streams<T>(a.src, a.dst, a.P.n);
+    if (kernel == KERNEL_STEP)
+        k_step<M, FM, OUT><<<grid, a.block, 0, a.stream>>>(a.P, S, out);
+    else
+        k_collide_local<M, FM, OUT><<<grid, a.block, 0, a.stream>>>(a.P, S, out);
+}
+
 template <int FM>
 static cudaError_t launch_exact_fm(int kernel, const LaunchArgs& a)
 {
     using M = ModeExact;
-    Outputs<double> out{(double*)a.rho, (double*)a.u, a.partials};
     const int grid = grid_for(a.P.n, a.block);
-    switch (kernel) {
-    case KERNEL_STEP:
-        k_step<M, FM><<<grid, a.block, 0, a.stream>>>(a.P, (const double*)a.src, (double*)a.dst, out);
-        break;
-    case KERNEL_COLLIDE_LOCAL:
-        k_collide_local<M, FM><<<grid, a.block, 0, a.stream>>>(a.P, (const double*)a.src, (double*)a.dst, out);
-        break;
-    case KERNEL_OBSERVE:
-        k_observe<M, FM><<<grid, a.block, 0, a.stream>>>(a.P, (const double*)a.src, a.post, a.f_out, out);
-        break;
-    default:
-        return cudaErrorInvalidValue;
+    if (kernel == KERNEL_OBSERVE) {
+        Outputs<double> out{(double*)a.rho, (double*)a.u, a.partials};
+        k_observe<M, FM><<<grid, a.block, 0, a.stream>>>(a.P, make_streams<double>(a.src, nullptr, a.P.n), a.post,
+                                                          a.f_out, out);
+        return cudaGetLastError();
+    }
+    if (kernel != KERNEL_STEP && kernel != KERNEL_COLLIDE_LOCAL) return cudaErrorInvalidValue;
+    switch (out_bits(a)) {
+    case OUT_NONE: launch_step_out<M, FM, OUT_NONE>(kernel, a, grid); break;
+    case OUT_RHO_U: launch_step_out<M, FM, OUT_RHO_U>(kernel, a, grid); break;
+    case OUT_SUMS: launch_step_out<M, FM, OUT_SUMS>(kernel, a, grid); break;
+    default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }
@@ -109,31 +121,30 @@ cudaError_t launch_feq_init(int storage, const Params& P, const double* rho, con
     }
 }
 
-__global__ void k_mark_near_solid(Params P, uint8_t* __restrict__ flags)
+__global__ void k_mark_near_solid(Params P, uint8_t* __restrict__ flags, uint32_t* __restrict__ bbmask)
 {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= P.n) return;
-    uint32_t xy = P.div_nz.div((uint32_t)idx);
-    const int z = idx - (int)xy * P.nz;
-    const uint32_t x = P.div_ny.div(xy);
-    const int y = (int)xy - (int)x * P.ny;
-    int fl = flags[idx] & 3;
-    if (fl != CELL_SOLID) {
-        const Nbr nb = make_nbr(P, (int)x, y, z);
-        bool near = false;
+    int x, y, z;
+    decode_xyz(P, idx, x, y, z);
+    const int type = flags[idx] & 3;
+    uint32_t mask = 0;
+    if (type != CELL_SOLID) {
+        const Nbr nb = make_nbr(P, x, y, z);
 #pragma unroll
-        for (int d = 1; d < Q; ++d) near |= (flags[nb.src(d)] & 3) == CELL_SOLID;
-        if (near) fl |= FLAG_NEAR_SOLID;
+        for (int d = 1; d < Q; ++d)
+            if ((flags[nb.src(d)] & 3) == CELL_SOLID) mask |= 1u << d;
     }
+    bbmask[idx] = mask;
     // Every thread reads only the low bits of its neighbours, so writing the
     // high bit in place is race-free.
-    flags[idx] = (uint8_t)((flags[idx] & 3) | (fl & FLAG_NEAR_SOLID));
+    flags[idx] = (uint8_t)(type | (mask ? FLAG_NEAR_SOLID : 0));
 }
 
-cudaError_t launch_mark_near_solid(const Params& P, uint8_t* flags, cudaStream_t s)
+cudaError_t launch_mark_near_solid(const Params& P, uint8_t* flags, uint32_t* bbmask, cudaStream_t s)
 {
     const int block = 256;
-    k_mark_near_solid<<<grid_for(P.n, block), block, 0, s>>>(P, flags);
+    k_mark_near_solid<<<grid_for(P.n, block), block, 0, s>>>(P, flags, bbmask);
     return cudaGetLastError();
 }
 
@@ -225,15 +236,6 @@ __global__ void k_ref_macro_u(Params P, const double* __restrict__ f, const doub
     }
 }
 
-__device__ __forceinline__ void decode_xyz(const Params& P, int idx, int& x, int& y, int& z)
-{
-    uint32_t xy = P.div_nz.div((uint32_t)idx);
-    z = idx - (int)xy * P.nz;
-    uint32_t xx = P.div_ny.div(xy);
-    y = (int)xy - (int)xx * P.ny;
-    x = (int)xx;
-}
-
 // _k_stream (d3q19_warp.py:198-212): out[d, x] = in[d, (x - c_d) mod n]
 __global__ void k_ref_stream(Params P, const double* __restrict__ fin, double* __restrict__ fout)
 {
@@ -263,8 +265,7 @@ __global__ void k_ref_bgk_step(Params P, const double* __restrict__ f, double* _
     const Nbr nb = make_nbr(P, x, y, z);
 #pragma unroll
     for (int d = 0; d < Q; ++d) {
-        const int dst = nb.X[1 + cx(d)] + nb.Y[1 + cy(d)] + nb.Z[1 + cz(d)];
-        fout[(size_t)d * P.n + dst] = fl[d];
+        fout[(size_t)d * P.n + nb.dst(d)] = fl[d];
     }
 }
 

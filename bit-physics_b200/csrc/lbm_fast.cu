@@ -5,24 +5,35 @@
 
 namespace lbm {
 
+template <class M, int FM, int OUT>
+static void launch_step_out(int kernel, const LaunchArgs& a, int grid)
+{
+    using T = typename M::T;
+    Outputs<float> out{(float*)a.rho, (float*)a.u, a.partials};
+    const Streams<T> S = make_streams<T>(a.src, a.dst, a.P.n);
+    if (kernel == KERNEL_STEP)
+        k_step<M, FM, OUT><<<grid, a.block, 0, a.stream>>>(a.P, S, out);
+    else
+        k_collide_local<M, FM, OUT><<<grid, a.block, 0, a.stream>>>(a.P, S, out);
+}
+
 template <class T, int FM>
 static cudaError_t launch_fast_t(int kernel, const LaunchArgs& a)
 {
     using M = ModeFast<T>;
-    Outputs<float> out{(float*)a.rho, (float*)a.u, a.partials};
     const int grid = grid_for(a.P.n, a.block);
-    switch (kernel) {
-    case KERNEL_STEP:
-        k_step<M, FM><<<grid, a.block, 0, a.stream>>>(a.P, (const T*)a.src, (T*)a.dst, out);
-        break;
-    case KERNEL_COLLIDE_LOCAL:
-        k_collide_local<M, FM><<<grid, a.block, 0, a.stream>>>(a.P, (const T*)a.src, (T*)a.dst, out);
-        break;
-    case KERNEL_OBSERVE:
-        k_observe<M, FM><<<grid, a.block, 0, a.stream>>>(a.P, (const T*)a.src, a.post, a.f_out, out);
-        break;
-    default:
-        return cudaErrorInvalidValue;
+    if (kernel == KERNEL_OBSERVE) {
+        Outputs<float> out{(float*)a.rho, (float*)a.u, a.partials};
+        k_observe<M, FM><<<grid, a.block, 0, a.stream>>>(a.P, make_streams<T>(a.src, nullptr, a.P.n), a.post,
+                                                          a.f_out, out);
+        return cudaGetLastError();
+    }
+    if (kernel != KERNEL_STEP && kernel != KERNEL_COLLIDE_LOCAL) return cudaErrorInvalidValue;
+    switch (out_bits(a)) {
+    case OUT_NONE: launch_step_out<M, FM, OUT_NONE>(kernel, a, grid); break;
+    case OUT_RHO_U: launch_step_out<M, FM, OUT_RHO_U>(kernel, a, grid); break;
+    case OUT_SUMS: launch_step_out<M, FM, OUT_SUMS>(kernel, a, grid); break;
+    default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }

@@ -3,7 +3,7 @@
 // State machine of a lattice (one storage buffer pair A/B):
 //   PRE   buffer holds f_n itself (after set_populations / set_equilibrium).
 //   POST  buffer holds P_{n-1} = collide(f_{n-1}); f_n = bounce(stream(P_{n-1}))
-//         is rebuilt on the fly by pull_state().
+//         is rebuilt on the fly by gather + resolve_state.
 // A step from PRE runs k_collide_local (read f_n in place, write P_n);
 // a step from POST runs k_step, the fused pull-stream + boundary + collide
 // kernel that reads P_{n-1} and writes P_n.  Either way the state advances
@@ -15,13 +15,16 @@
 
 namespace lbm {
 
-// Optional outputs of a kernel: rho/u readback of the pre-collision state and
-// per-block FP64 conservation partials.  Null pointers disable them.
+// What a kernel writes besides the populations (template parameter OUT).
+enum OutBits : int { OUT_NONE = 0, OUT_RHO_U = 1, OUT_SUMS = 2 };
+
+// Optional outputs: rho/u readback of the pre-collision state and per-block
+// FP64 conservation partials (mass or mass deviation, m_x, m_y, m_z, cells).
 template <class C>
 struct Outputs {
-    C* rho;          // (n)
-    C* u;            // (3, n)
-    double* partials; // (gridDim.x, 5): mass, mx, my, mz, fluid-cell count
+    C* rho;           // (n)
+    C* u;             // (3, n)
+    double* partials; // (gridDim.x, 5)
 };
 
 // Block-level FP64 reduction of 5 values, fixed tree (deterministic for a
@@ -52,64 +55,75 @@ __device__ __forceinline__ void block_sum5(double v[5], double* out)
     }
 }
 
-template <class M, int FM>
+template <class M, int FM, int OUT>
 __device__ __forceinline__ void emit(const Params& P, const Outputs<typename M::C>& out, int idx, bool solid,
-                                     const typename M::C* f, double cons[5])
+                                     const typename M::C* f, double* cons)
 {
     using C = typename M::C;
-    if (out.rho) {
-        if (solid) {
-            out.rho[idx] = C(0);
-            out.u[idx] = C(0);
-            out.u[P.n + idx] = C(0);
-            out.u[2 * P.n + idx] = C(0);
-        } else {
-            C r, u[3];
-            M::template readback<FM>(P, idx, f, r, u);
-            out.rho[idx] = r;
-            out.u[idx] = u[0];
-            out.u[P.n + idx] = u[1];
-            out.u[2 * P.n + idx] = u[2];
-        }
+    if constexpr ((OUT & OUT_RHO_U) != 0) {
+        C r = C(0), u[3] = {C(0), C(0), C(0)};
+        if (!solid) M::template readback<FM>(P, idx, f, r, u);
+        out.rho[idx] = r;
+        out.u[idx] = u[0];
+        out.u[P.n + idx] = u[1];
+        out.u[2 * P.n + idx] = u[2];
     }
-    if (out.partials && !solid) {
-        double m, a, b, c;
-        M::cons_terms(f, m, a, b, c);
-        cons[0] += m; cons[1] += a; cons[2] += b; cons[3] += c; cons[4] += 1.0;
+    if constexpr ((OUT & OUT_SUMS) != 0) {
+        if (!solid) {
+            double m, a, b, c;
+            M::cons_terms(f, m, a, b, c);
+            cons[0] += m; cons[1] += a; cons[2] += b; cons[3] += c; cons[4] += 1.0;
+        }
     }
 }
 
-// Fused step from POST: f_n = pull_state(P_{n-1}); optional readback of f_n;
-// P_n = collide(f_n) -> dst.  Solid cells store their rest value.
-template <class M, int FM>
-__global__ void __launch_bounds__(512) k_step(Params P, const typename M::T* __restrict__ src,
-                                              typename M::T* __restrict__ dst, Outputs<typename M::C> out)
+template <class M>
+__device__ __forceinline__ void store_all(const Streams<typename M::T>& S, int idx, const typename M::C* f)
+{
+#pragma unroll
+    for (int d = 0; d < Q; ++d) M::store(S.dst[d] + idx, d, f[d]);
+}
+
+template <class M>
+__device__ __forceinline__ void store_solid(const Params& P, const Streams<typename M::T>& S, int idx)
+{
+#pragma unroll
+    for (int d = 0; d < Q; ++d) M::store(S.dst[d] + idx, d, M::solid(P, d));
+}
+
+// Fused step from POST: f_n = gather + resolve_state(P_{n-1}); optional
+// outputs of f_n; P_n = collide(f_n).  Solid cells store their rest value.
+// The own-position gather is issued before the flag byte is examined, so the
+// 19 loads and the flag load are in flight together.
+template <class M, int FM, int OUT>
+__global__ void __launch_bounds__(256) k_step(Params P, Streams<typename M::T> S, Outputs<typename M::C> out)
 {
     using C = typename M::C;
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     double cons[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     if (idx < P.n) {
-        const Site s = decode_site(P, idx);
+        int x, y, z;
+        decode_xyz(P, idx, x, y, z);
+        const int fl = P.has_flags ? (int)P.flags[idx] : 0;
+        const Nbr nb = make_nbr(P, x, y, z);
         C f[Q];
-        if (s.type == CELL_SOLID) {
-            emit<M, FM>(P, out, idx, true, f, cons);
-#pragma unroll
-            for (int d = 0; d < Q; ++d) M::store(dst + (size_t)d * P.n + idx, d, M::solid(P, d));
-        } else {
-            pull_state<M>(P, src, s, f);
-            emit<M, FM>(P, out, idx, false, f, cons);
+        gather<M>(S, nb, f);
+        if (resolve_state<M>(P, S, idx, x, y, z, fl, nb, f)) {
+            emit<M, FM, OUT>(P, out, idx, false, f, cons);
             M::template collide<FM>(P, idx, f);
-#pragma unroll
-            for (int d = 0; d < Q; ++d) M::store(dst + (size_t)d * P.n + idx, d, f[d]);
+            store_all<M>(S, idx, f);
+        } else {
+            emit<M, FM, OUT>(P, out, idx, true, f, cons);
+            store_solid<M>(P, S, idx);
         }
     }
-    if (out.partials) block_sum5(cons, out.partials);
+    if constexpr ((OUT & OUT_SUMS) != 0) block_sum5(cons, out.partials);
 }
 
-// Step from PRE: read f_n in place, collide, write P_n.
-template <class M, int FM>
-__global__ void __launch_bounds__(512) k_collide_local(Params P, const typename M::T* __restrict__ src,
-                                                       typename M::T* __restrict__ dst,
+// Step from PRE: read f_n in place, collide, write P_n.  S.src holds the
+// buffer base pointers (direction d at S.src[d]).
+template <class M, int FM, int OUT>
+__global__ void __launch_bounds__(256) k_collide_local(Params P, Streams<typename M::T> S,
                                                        Outputs<typename M::C> out)
 {
     using C = typename M::C;
@@ -118,28 +132,26 @@ __global__ void __launch_bounds__(512) k_collide_local(Params P, const typename 
     if (idx < P.n) {
         const int type = P.has_flags ? (P.flags[idx] & 3) : CELL_FLUID;
         C f[Q];
+#pragma unroll
+        for (int d = 0; d < Q; ++d) f[d] = M::load(S.src[d] + idx, d);
         if (type == CELL_SOLID) {
-            emit<M, FM>(P, out, idx, true, f, cons);
-#pragma unroll
-            for (int d = 0; d < Q; ++d) M::store(dst + (size_t)d * P.n + idx, d, M::solid(P, d));
+            emit<M, FM, OUT>(P, out, idx, true, f, cons);
+            store_solid<M>(P, S, idx);
         } else {
-#pragma unroll
-            for (int d = 0; d < Q; ++d) f[d] = M::load(src + (size_t)d * P.n + idx, d);
-            emit<M, FM>(P, out, idx, false, f, cons);
+            emit<M, FM, OUT>(P, out, idx, false, f, cons);
             M::template collide<FM>(P, idx, f);
-#pragma unroll
-            for (int d = 0; d < Q; ++d) M::store(dst + (size_t)d * P.n + idx, d, f[d]);
+            store_all<M>(S, idx, f);
         }
     }
-    if (out.partials) block_sum5(cons, out.partials);
+    if constexpr ((OUT & OUT_SUMS) != 0) block_sum5(cons, out.partials);
 }
 
-// Current state without advancing it: f_n (f64, optional; used for POST
+// Current state without advancing it: f_n as f64 (optional; used for POST
 // states -- a PRE buffer is read out exactly by k_load_f64), readback and
 // conservation partials.  post = true rebuilds f_n from P_{n-1}; false reads
 // the PRE buffer in place.
 template <class M, int FM>
-__global__ void __launch_bounds__(512) k_observe(Params P, const typename M::T* __restrict__ src, bool post,
+__global__ void __launch_bounds__(256) k_observe(Params P, Streams<typename M::T> S, bool post,
                                                  double* __restrict__ f_out, Outputs<typename M::C> out)
 {
     using C = typename M::C;
@@ -148,25 +160,28 @@ __global__ void __launch_bounds__(512) k_observe(Params P, const typename M::T* 
     if (idx < P.n) {
         C f[Q];
         bool solid;
+        const int fl = P.has_flags ? (int)P.flags[idx] : 0;
         if (post) {
-            const Site s = decode_site(P, idx);
-            solid = s.type == CELL_SOLID;
+            int x, y, z;
+            decode_xyz(P, idx, x, y, z);
+            const Nbr nb = make_nbr(P, x, y, z);
+            gather<M>(S, nb, f);
+            solid = !resolve_state<M>(P, S, idx, x, y, z, fl, nb, f);
             if (solid) {
 #pragma unroll
                 for (int d = 0; d < Q; ++d) f[d] = M::solid(P, d);
-            } else {
-                pull_state<M>(P, src, s, f);
             }
         } else {
-            solid = P.has_flags && (P.flags[idx] & 3) == CELL_SOLID;
+            solid = (fl & 3) == CELL_SOLID;
 #pragma unroll
-            for (int d = 0; d < Q; ++d) f[d] = M::load(src + (size_t)d * P.n + idx, d);
+            for (int d = 0; d < Q; ++d) f[d] = M::load(S.src[d] + idx, d);
         }
         if (f_out) {
 #pragma unroll
             for (int d = 0; d < Q; ++d) f_out[(size_t)d * P.n + idx] = M::to_f64(P, d, f[d]);
         }
-        emit<M, FM>(P, out, idx, solid, f, cons);
+        if (out.rho) emit<M, FM, OUT_RHO_U>(P, out, idx, solid, f, cons);
+        if (out.partials) emit<M, FM, OUT_SUMS>(P, out, idx, solid, f, cons);
     }
     if (out.partials) block_sum5(cons, out.partials);
 }
@@ -213,7 +228,21 @@ __global__ void k_feq_init(Params P, const double* __restrict__ rho, const doubl
     }
 }
 
-// Mark fluid / inflow / outflow cells that pull from a solid cell.
-__global__ void k_mark_near_solid(Params P, uint8_t* __restrict__ flags);
+// Bounce-back masks: for every non-solid cell, bit d set when its pull
+// source x - c_d is solid; the flag byte's FLAG_NEAR_SOLID bit mirrors
+// mask != 0.
+__global__ void k_mark_near_solid(Params P, uint8_t* __restrict__ flags, uint32_t* __restrict__ bbmask);
+
+// Per-direction base pointers of a population buffer of n cells.
+template <class T>
+inline Streams<T> make_streams(const void* src, void* dst, int n)
+{
+    Streams<T> S;
+    for (int d = 0; d < Q; ++d) {
+        S.src[d] = src ? (const T*)src + (size_t)d * n : nullptr;
+        S.dst[d] = dst ? (T*)dst + (size_t)d * n : nullptr;
+    }
+    return S;
+}
 
 }  // namespace lbm

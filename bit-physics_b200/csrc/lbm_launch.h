@@ -25,6 +25,10 @@ struct LaunchArgs {
     cudaStream_t stream;
 };
 
+// Output selection of a step launch (OUT_* bits of lbm_kernels.cuh) from the
+// optional pointers: rho/u and partials are mutually exclusive for steps.
+inline int out_bits(const LaunchArgs& a) { return (a.rho ? 1 : 0) | (a.partials ? 2 : 0); }
+
 inline int grid_for(long long work, int block) { return (int)((work + block - 1) / block); }
 
 // Stateful engine kernels.
@@ -34,7 +38,7 @@ cudaError_t launch_store_f64(int storage, const Params& P, const double* f, void
 cudaError_t launch_load_f64(int storage, const Params& P, const void* src, double* f, cudaStream_t s);
 cudaError_t launch_feq_init(int storage, const Params& P, const double* rho, const double* u, void* dst,
                             cudaStream_t s);
-cudaError_t launch_mark_near_solid(const Params& P, uint8_t* flags, cudaStream_t s);
+cudaError_t launch_mark_near_solid(const Params& P, uint8_t* flags, uint32_t* bbmask, cudaStream_t s);
 cudaError_t launch_reduce_partials(const double* partials, int nblocks, double* out5, cudaStream_t s);
 
 // Stateless reference functions (f64, bit-exact), device pointers.

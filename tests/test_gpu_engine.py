@@ -97,7 +97,7 @@ def test_f64_block_sizes_agree():
     shape = (13, 11, 7)
     f0 = random_state(shape, 21)
     outs = []
-    for bs in (32, 128, 512):
+    for bs in (32, 96, 256):
         gpu, _ = pair(shape, 0.7, periodic=(False, True, True), block_size=bs)
         with gpu:
             gpu.set_populations(f0)
