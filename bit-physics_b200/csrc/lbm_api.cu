@@ -14,8 +14,16 @@
 using namespace lbm;
 
 namespace {
-
 thread_local std::string g_err;
+}  // namespace
+
+int lbm::set_error(int code, const char* message)
+{
+    g_err = message ? message : "";
+    return code;
+}
+
+namespace {
 
 int fail(int code, const char* fmt, ...)
 {

@@ -41,6 +41,9 @@ cudaError_t launch_feq_init(int storage, const Params& P, const double* rho, con
 cudaError_t launch_mark_near_solid(const Params& P, uint8_t* flags, uint32_t* bbmask, cudaStream_t s);
 cudaError_t launch_reduce_partials(const double* partials, int nblocks, double* out5, cudaStream_t s);
 
+// Record the calling thread's error message (lbm_last_error) and return code.
+int set_error(int code, const char* message);
+
 // Stateless reference functions (f64, bit-exact), device pointers.
 cudaError_t ref_feq_field(const Params& P, const double* rho, const double* u, double* feq, cudaStream_t s);
 cudaError_t ref_density(const Params& P, const double* f, double* rho, cudaStream_t s);

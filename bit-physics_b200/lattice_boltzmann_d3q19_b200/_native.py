@@ -99,6 +99,7 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "lbm_stream_dev": ([_h, _h, _i, _i, _i, _h], C.c_int),
     "lbm_bgk_step_dev": ([_h, _h, C.c_double, _h, _i, _i, _i, _h], C.c_int),
     "lbm_bounce_back_y_walls_dev": ([_h, _h, _i, _i, _i, _dp, _dp, _h], C.c_int),
+    "lbm_conservation_noalloc": ([_h, _h, _i, _i, _i, _h, _h], C.c_int),
     "lbm_last_error": ([], C.c_char_p),
     "lbm_version": ([], C.c_int),
     "lbm_device_count": ([], C.c_int),

@@ -185,6 +185,22 @@ int lbm_bounce_back_y_walls_dev(const double* f, double* f_out, int32_t nx, int3
                                 int32_t nz, const double* wall_velocity_top,
                                 const double* wall_velocity_bottom, void* stream);
 
+/* ---- without device allocation ----------------------------------------- */
+/* No counterpart in the reference.  FP64 sums {sum rho, sum m_x, sum m_y,
+ * sum m_z} of a population array f (19, nx, ny, nz, f64, device memory) over
+ * its non-solid cells (flags: optional device uint8 cell types), written to
+ * out4 (4 doubles, device memory), enqueued on `stream` (NULL: the legacy
+ * default stream).  The same reduction as lbm_conservation on a lattice
+ * holding f, but it allocates nothing: its scratch is one fixed device array
+ * per GPU, for callers that cannot call cudaMalloc where they need the sums
+ * (another allocator owns the device memory, or a step loop must not be
+ * stalled by an allocation).  At most LBM_NOALLOC_MAX_CELLS cells; calls that
+ * overlap on one GPU race on the shared array.  The first call on a device
+ * looks up the array's address and should come before any stream capture. */
+#define LBM_NOALLOC_MAX_CELLS 16777216LL
+int lbm_conservation_noalloc(const double* f, const uint8_t* flags, int32_t nx, int32_t ny, int32_t nz,
+                             double* out4, void* stream);
+
 /* ---- library ------------------------------------------------------------ */
 const char* lbm_last_error(void);
 int lbm_version(void);
