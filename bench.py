@@ -164,10 +164,14 @@ def channel_geometry():
     return flags
 
 
+CELLS_PER_THREAD = 0  # 0: the library's choice
+
+
 def make_lattice(storage: str, flags, device: int):
     from lattice_boltzmann_d3q19_b200 import Lattice
 
-    lat = Lattice(SHAPE, TAU, storage=storage, inflow_u=(INFLOW_U, 0.0, 0.0), device=device)
+    lat = Lattice(SHAPE, TAU, storage=storage, inflow_u=(INFLOW_U, 0.0, 0.0), device=device,
+                  cells_per_thread=CELLS_PER_THREAD)
     lat.set_flags(flags)
     lat.set_equilibrium(1.0, (INFLOW_U, 0.0, 0.0))
     return lat
@@ -350,7 +354,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         del u0
         from lattice_boltzmann_d3q19_b200 import Lattice
 
-        lat = Lattice(SHAPE, TAU, storage=args.storage, inflow_u=(INFLOW_U, 0.0, 0.0), device=dev)
+        lat = Lattice(SHAPE, TAU, storage=args.storage, inflow_u=(INFLOW_U, 0.0, 0.0), device=dev,
+                      cells_per_thread=CELLS_PER_THREAD)
         lat.set_populations(f0_pinned)  # allocate staging outside the timed region
         torch.cuda.synchronize()
         if dist_on:
@@ -434,7 +439,10 @@ def main():
     ap.add_argument("--skip-variants", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--cells-per-thread", type=int, default=0, choices=[0, 1, 2])
     args = ap.parse_args()
+    global CELLS_PER_THREAD
+    CELLS_PER_THREAD = args.cells_per_thread
     if args.warmup < 3 and args.impl == "ours":
         ap.error("--warmup must be >= 3")
     rank = int(os.environ.get("RANK", "0"))

@@ -79,6 +79,7 @@ struct Params {
     int nx, ny, nz, n, nynz;
     FastDiv div_nz, div_ny;
     int periodic;      // bit 0 x, 1 y, 2 z
+    unsigned walled[3]; // 1 where the axis is not periodic
     int has_flags;
     int wall_sum_pairwise; // nx * nz == 1 (see ModeExact::rho_wall)
     const uint8_t* flags;
@@ -113,6 +114,54 @@ __device__ __forceinline__ float ld_dev(const __nv_bfloat16* p, int) { return __
 __device__ __forceinline__ void st_dev(float* p, int d, float h) { *p = h + wf(d); }
 __device__ __forceinline__ void st_dev(__half* p, int, float h) { *p = __float2half_rn(h); }
 __device__ __forceinline__ void st_dev(__nv_bfloat16* p, int, float h) { *p = __float2bfloat16_rn(h); }
+// Two consecutive elements (z, z+1) at an 8-byte (f32) / 4-byte (16-bit)
+// aligned address, as deviations from the weight.
+__device__ __forceinline__ void ld_dev2(const float* p, int d, float& a, float& b)
+{
+    const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+    a = v.x - wf(d);
+    b = v.y - wf(d);
+}
+__device__ __forceinline__ void ld_dev2(const __half* p, int, float& a, float& b)
+{
+    const float2 v = __half22float2(__ldg(reinterpret_cast<const __half2*>(p)));
+    a = v.x;
+    b = v.y;
+}
+__device__ __forceinline__ void ld_dev2(const __nv_bfloat16* p, int, float& a, float& b)
+{
+    const float2 v = __bfloat1622float2(__ldg(reinterpret_cast<const __nv_bfloat162*>(p)));
+    a = v.x;
+    b = v.y;
+}
+__device__ __forceinline__ void st_dev2(float* p, int d, float a, float b)
+{
+    *reinterpret_cast<float2*>(p) = make_float2(a + wf(d), b + wf(d));
+}
+__device__ __forceinline__ void st_dev2(__half* p, int, float a, float b)
+{
+    *reinterpret_cast<__half2*>(p) = __floats2half2_rn(a, b);
+}
+__device__ __forceinline__ void st_dev2(__nv_bfloat16* p, int, float a, float b)
+{
+    *reinterpret_cast<__nv_bfloat162*>(p) = __floats2bfloat162_rn(a, b);
+}
+// Packed two-lane f32 arithmetic (sm_100 FFMA2 / FADD2 / FMUL2): lane x is
+// cell z, lane y cell z + 1.  Every operation is correctly rounded per lane.
+__device__ __forceinline__ float2 bc2(float s) { return make_float2(s, s); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, bc2(-1.0f), a); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+// Two scalar population values (cells z, z + 1 of one direction, stored at
+// unrelated addresses) as deviations.
+template <class T>
+__device__ __forceinline__ float2 ld_dev_pair(const T* pa, const T* pb, int d)
+{
+    return make_float2(ld_dev(pa, d), ld_dev(pb, d));
+}
+
 // f64 value -> storage, rounding as the oracle's store_round does.
 __device__ __forceinline__ void st_f64(double* p, int, double v, const Params&) { *p = v; }
 __device__ __forceinline__ void st_f64(float* p, int, double v, const Params&) { *p = (float)v; }
@@ -170,7 +219,7 @@ __device__ __forceinline__ void force_fast(const Params& P, int cell, float mx, 
         Fx = __ldg(F + cell); Fy = __ldg(F + P.n + cell); Fz = __ldg(F + 2 * P.n + cell);
     } else if (FM == FORCE_DRAG) {
         float ka = P.drag_kf * __ldg(P.porosity + cell);
-        float beta = ka / (1.0f + 0.5f * ka);
+        float beta = __fdividef(ka, 1.0f + 0.5f * ka);
         Fx = P.body_force_f[0] - beta * mx;
         Fy = P.body_force_f[1] - beta * my;
         Fz = P.body_force_f[2] - beta * mz;
@@ -195,7 +244,8 @@ struct ModeExact {
     // sum_d f[d] of the raw (pre-bounce) gather, bgk.py:203 / :212.  NumPy
     // reduces a wall row in lex order, except when the row is a single cell
     // (nx * nz == 1): then it runs its 8-accumulator pairwise summation.
-    static __device__ __forceinline__ C rho_wall(const Params& P, const C* f)
+    template <class F>
+    static __device__ __forceinline__ C rho_wall(const Params& P, const F& f)
     {
         if (!P.wall_sum_pairwise) {
             double r = 0.0;
@@ -327,7 +377,8 @@ struct ModeFast {
         else return P.w[d] + (double)h;
     }
 
-    static __device__ __forceinline__ C rho_wall(const Params&, const C* h)
+    template <class F>
+    static __device__ __forceinline__ C rho_wall(const Params&, const F& h)
     {
         float r = 0.0f;
 #pragma unroll
@@ -357,7 +408,7 @@ struct ModeFast {
             if (cz(d) == 1) mz += h[d]; else if (cz(d) == -1) mz -= h[d];
         }
         float rho = 1.0f + rd;
-        float inv = 1.0f / rho_safe(rho);
+        float inv = __fdividef(1.0f, rho_safe(rho));
         float Fx, Fy, Fz;
         force_fast<FM>(P, cell, mx, my, mz, Fx, Fy, Fz);
         float ux, uy, uz;
@@ -391,6 +442,93 @@ struct ModeFast {
             }
             h[d] = hd;
             h[o] = ho;
+        }
+    }
+
+    // The same collision for two cells at once (lanes of float2), in packed
+    // f32x2 arithmetic; force fields / porosity are read as (cell, cell + 1)
+    // pairs, so cell0 must be even.  Opposite directions are paired through
+    // p_d = h_d - h_opp(d) for the momentum sums.  sink(d, value) receives
+    // each direction's post-collision pair as soon as it is final.
+    template <int FM, class Sink>
+    static __device__ __forceinline__ void collide2(const Params& P, int cell0, float2* h, Sink&& sink)
+    {
+        float2 rd = h[0];
+#pragma unroll
+        for (int d = 1; d < Q; ++d) rd = add2(rd, h[d]);
+        const float2 p1 = sub2(h[1], h[2]), p3 = sub2(h[3], h[4]), p5 = sub2(h[5], h[6]);
+        const float2 p7 = sub2(h[7], h[8]), p9 = sub2(h[9], h[10]), p11 = sub2(h[11], h[12]);
+        const float2 p13 = sub2(h[13], h[14]), p15 = sub2(h[15], h[16]), p17 = sub2(h[17], h[18]);
+        const float2 mx = add2(add2(add2(p1, p7), add2(p9, p11)), p13);
+        const float2 my = add2(add2(sub2(add2(p3, p7), p9), p15), p17);
+        const float2 mz = sub2(add2(sub2(add2(p5, p11), p13), p15), p17);
+        const float2 rho = add2(rd, bc2(1.0f));
+        const float2 inv = make_float2(__fdividef(1.0f, rho_safe(rho.x)), __fdividef(1.0f, rho_safe(rho.y)));
+        float2 Fx = bc2(0.0f), Fy = bc2(0.0f), Fz = bc2(0.0f);
+        if constexpr (FM == FORCE_UNIFORM) {
+            Fx = bc2(P.body_force_f[0]); Fy = bc2(P.body_force_f[1]); Fz = bc2(P.body_force_f[2]);
+        } else if constexpr (FM == FORCE_FIELD) {
+            const float* F = (const float*)P.force;
+            Fx = __ldg(reinterpret_cast<const float2*>(F + cell0));
+            Fy = __ldg(reinterpret_cast<const float2*>(F + P.n + cell0));
+            Fz = __ldg(reinterpret_cast<const float2*>(F + 2 * P.n + cell0));
+        } else if constexpr (FM == FORCE_DRAG) {
+            const float2 a = __ldg(reinterpret_cast<const float2*>(P.porosity + cell0));
+            const float2 ka = mul2(bc2(P.drag_kf), a);
+            const float2 den = fma2(bc2(0.5f), ka, bc2(1.0f));
+            const float2 nbeta = make_float2(-__fdividef(ka.x, den.x), -__fdividef(ka.y, den.y));
+            Fx = fma2(nbeta, mx, bc2(P.body_force_f[0]));
+            Fy = fma2(nbeta, my, bc2(P.body_force_f[1]));
+            Fz = fma2(nbeta, mz, bc2(P.body_force_f[2]));
+        }
+        float2 ux, uy, uz;
+        if constexpr (FM == FORCE_NONE) {
+            ux = mul2(mx, inv); uy = mul2(my, inv); uz = mul2(mz, inv);
+        } else {
+            ux = mul2(fma2(bc2(0.5f), Fx, mx), inv);
+            uy = mul2(fma2(bc2(0.5f), Fy, my), inv);
+            uz = mul2(fma2(bc2(0.5f), Fz, mz), inv);
+        }
+        const float2 usq = fma2(uz, uz, fma2(uy, uy, mul2(ux, ux)));
+        const float2 base = fma2(rho, mul2(usq, bc2(-1.5f)), rd);  // rho_dev - 1.5 rho u^2
+        const float om = P.omega;
+        const float2 keep = bc2(1.0f - om);
+        const float2 rho45 = mul2(rho, bc2(4.5f));
+        const float2 asym18 = mul2(rho, bc2(3.0f * om * wf(1)));
+        const float2 asym36 = mul2(rho, bc2(3.0f * om * wf(7)));
+        float2 nuF3 = bc2(0.0f);
+        if constexpr (FM != FORCE_NONE) nuF3 = mul2(bc2(-3.0f), fma2(uz, Fz, fma2(uy, Fy, mul2(ux, Fx))));
+        // rest direction
+        h[0] = fma2(keep, h[0], mul2(bc2(om * wf(0)), base));
+        if constexpr (FM != FORCE_NONE) h[0] = fma2(bc2(P.pref * wf(0)), nuF3, h[0]);
+        sink(0, h[0]);
+#pragma unroll
+        for (int d = 1; d < Q; d += 2) {
+            float2 cu, cF;
+            switch (d) {
+            case 1: cu = ux; cF = Fx; break;
+            case 3: cu = uy; cF = Fy; break;
+            case 5: cu = uz; cF = Fz; break;
+            case 7: cu = add2(ux, uy); cF = add2(Fx, Fy); break;
+            case 9: cu = sub2(ux, uy); cF = sub2(Fx, Fy); break;
+            case 11: cu = add2(ux, uz); cF = add2(Fx, Fz); break;
+            case 13: cu = sub2(ux, uz); cF = sub2(Fx, Fz); break;
+            case 15: cu = add2(uy, uz); cF = add2(Fy, Fz); break;
+            default: cu = sub2(uy, uz); cF = sub2(Fy, Fz); break;
+            }
+            const float w = wf(d);
+            const float2 s1 = fma2(mul2(rho45, cu), cu, base);       // rho_dev + rho(4.5 cu^2 - 1.5 u^2)
+            float2 sym = mul2(bc2(om * w), s1);
+            float2 asym = mul2(d < 7 ? asym18 : asym36, cu);          // om 3 w rho cu
+            if constexpr (FM != FORCE_NONE) {
+                const float pw = P.pref * w;
+                sym = fma2(bc2(pw), fma2(mul2(bc2(9.0f), cu), cF, nuF3), sym);  // + pref w (9 cu cF - 3 u.F)
+                asym = fma2(bc2(3.0f * pw), cF, asym);                            // + pref w 3 c.F
+            }
+            h[d] = fma2(keep, h[d], add2(sym, asym));
+            h[d + 1] = fma2(keep, h[d + 1], sub2(sym, asym));
+            sink(d, h[d]);
+            sink(d + 1, h[d + 1]);
         }
     }
 
@@ -475,11 +613,13 @@ __device__ __forceinline__ void decode_xyz(const Params& P, int idx, int& x, int
     x = (int)xx;
 }
 
+// Branch-free: the cell lies on a face of a walled (non-periodic) axis.
 __device__ __forceinline__ bool on_walled_face(const Params& P, int gx, int y, int z)
 {
-    return (!(P.periodic & 1) && (gx == 0 || gx == P.nx - 1)) ||
-           (!(P.periodic & 2) && (y == 0 || y == P.ny - 1)) ||
-           (!(P.periodic & 4) && (z == 0 || z == P.nz - 1));
+    const unsigned ex = (unsigned)(gx == 0) | (unsigned)(gx == P.nx - 1);
+    const unsigned ey = (unsigned)(y == 0) | (unsigned)(y == P.ny - 1);
+    const unsigned ez = (unsigned)(z == 0) | (unsigned)(z == P.nz - 1);
+    return ((ex & P.walled[0]) | (ey & P.walled[1]) | (ez & P.walled[2])) != 0u;
 }
 
 // Walled face crossed by the pull source of direction d, or -1.  Priority when
@@ -496,9 +636,17 @@ __device__ __forceinline__ int crossed_face(const Params& P, int d, int gx, int 
     return -1;
 }
 
+// One lane (cell) of an array of float2 pairs, indexable like a float array;
+// lets the scalar boundary code work in place on two-cell state.
+template <int L>
+struct Lane {
+    float2* h;
+    __device__ __forceinline__ float& operator[](int d) const { return L ? h[d].y : h[d].x; }
+};
+
 // Raw pull of all 19 directions at the position described by nb.
-template <class M>
-__device__ __forceinline__ void gather(const Streams<typename M::T>& S, const Nbr& nb, typename M::C* f)
+template <class M, class F>
+__device__ __forceinline__ void gather(const Streams<typename M::T>& S, const Nbr& nb, F&& f)
 {
 #pragma unroll
     for (int d = 0; d < Q; ++d) f[d] = M::load(S.src[d] + nb.src(d), d);
@@ -510,10 +658,10 @@ __device__ __forceinline__ void gather(const Streams<typename M::T>& S, const Nb
 // does (bgk.py:190-216 reads its input f and writes a copy).
 //   walled face crossed:  f[d] = raw[opp(d)] + injection(face, rho_w)
 //   solid source (mask):  f[d] = P[opp(d)] at the cell (half-way bounce-back)
-template <class M>
+template <class M, class F>
 __device__ __forceinline__ void boundary_fix(const Params& P, const Streams<typename M::T>& S, const Nbr& nb,
                                              int gx, int y, int z, int gidx, bool face_cell, uint32_t bbmask,
-                                             typename M::C* f)
+                                             F&& f)
 {
     using C = typename M::C;
     C rho_w = C(0);
@@ -537,12 +685,12 @@ __device__ __forceinline__ void boundary_fix(const Params& P, const Streams<type
 //                  treated as fluid)
 //   fluid cell:    boundary_fix where it sits on a walled face or pulls from
 //                  a solid cell
-template <class M>
+template <class M, class F>
 __device__ __forceinline__ bool resolve_state(const Params& P, const Streams<typename M::T>& S, int idx, int x,
-                                              int y, int z, int fl, const Nbr& nb, typename M::C* f)
+                                              int y, int z, int fl, const Nbr& nb, F&& f)
 {
     const bool face = on_walled_face(P, x, y, z);
-    if (fl == 0 && !face) return true;
+    if ((fl | (int)face) == 0) return true;
     const int type = fl & 3;
     if (type == CELL_SOLID) return false;
     if (type == CELL_INFLOW) {

@@ -26,6 +26,7 @@ static void launch_step_out(int kernel, const LaunchArgs& a, int grid)
         k_step<M, FM, OUT><<<grid, a.block, 0, a.stream>>>(a.P, S, out);
     else
         k_collide_local<M, FM, OUT><<<grid, a.block, 0, a.stream>>>(a.P, S, out);
+    if (a.grid_used) *a.grid_used = grid;
 }
 
 template <int FM>

@@ -11,10 +11,17 @@ static void launch_step_out(int kernel, const LaunchArgs& a, int grid)
     using T = typename M::T;
     Outputs<float> out{(float*)a.rho, (float*)a.u, a.partials};
     const Streams<T> S = make_streams<T>(a.src, a.dst, a.P.n);
+    if (kernel == KERNEL_STEP && a.vec == 2) {
+        const int grid2 = grid_for(a.P.n / 2, a.block);
+        k_step2<M, FM, OUT><<<grid2, a.block, 0, a.stream>>>(a.P, S, out);
+        if (a.grid_used) *a.grid_used = grid2;
+        return;
+    }
     if (kernel == KERNEL_STEP)
         k_step<M, FM, OUT><<<grid, a.block, 0, a.stream>>>(a.P, S, out);
     else
         k_collide_local<M, FM, OUT><<<grid, a.block, 0, a.stream>>>(a.P, S, out);
+    if (a.grid_used) *a.grid_used = grid;
 }
 
 template <class T, int FM>
@@ -29,6 +36,7 @@ static cudaError_t launch_fast_t(int kernel, const LaunchArgs& a)
         return cudaGetLastError();
     }
     if (kernel != KERNEL_STEP && kernel != KERNEL_COLLIDE_LOCAL) return cudaErrorInvalidValue;
+    if (a.vec == 2 && (a.P.nz % 2) != 0) return cudaErrorInvalidValue;
     switch (out_bits(a)) {
     case OUT_NONE: launch_step_out<M, FM, OUT_NONE>(kernel, a, grid); break;
     case OUT_RHO_U: launch_step_out<M, FM, OUT_RHO_U>(kernel, a, grid); break;

@@ -13,6 +13,10 @@
 
 #include "lbm_device.cuh"
 
+#ifndef LBM_STEP2_MIN_BLOCKS
+#define LBM_STEP2_MIN_BLOCKS 3
+#endif
+
 namespace lbm {
 
 // What a kernel writes besides the populations (template parameter OUT).
@@ -116,6 +120,69 @@ __global__ void __launch_bounds__(256) k_step(Params P, Streams<typename M::T> S
             emit<M, FM, OUT>(P, out, idx, true, f, cons);
             store_solid<M>(P, S, idx);
         }
+    }
+    if constexpr ((OUT & OUT_SUMS) != 0) block_sum5(cons, out.partials);
+}
+
+// Fused step from POST, two z-adjacent cells (z0 even, z0 + 1) per thread, for
+// the f32-arithmetic storages; requires nz even (both cells share a row, rows
+// start at even indices).  Both cells' values of a direction live in one
+// float2 and the collision runs in packed f32x2 arithmetic (one FFMA2 / FADD2
+// per operation for the two cells).  The 9 directions with c_z = 0 pull both
+// values with one vector load, the 10 z-shifted ones with two scalar loads;
+// all 19 stores are vector stores.  Cells that need a boundary rule are
+// resolved one at a time with k_step's scalar resolve_state.
+template <class M, int FM, int OUT>
+__global__ void __launch_bounds__(256, LBM_STEP2_MIN_BLOCKS) k_step2(Params P, Streams<typename M::T> S, Outputs<typename M::C> out)
+{
+    using T = typename M::T;
+    const int idx0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+    double cons[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (idx0 < P.n) {
+        int x, y, z0;
+        decode_xyz(P, idx0, x, y, z0);
+        int fl0 = 0, fl1 = 0;
+        if (P.has_flags) {
+            const unsigned short both = __ldg(reinterpret_cast<const unsigned short*>(P.flags + idx0));
+            fl0 = both & 0xff;
+            fl1 = both >> 8;
+        }
+        const Nbr nb0 = make_nbr(P, x, y, z0);
+        const int zp1 = z0 + 2 == P.nz ? 0 : z0 + 2; // (z0 + 1) + 1, wrapped
+        float2 h[Q];
+#pragma unroll
+        for (int d = 0; d < Q; ++d) {
+            const T* p = S.src[d] + nb0.X[1 - cx(d)] + nb0.Y[1 - cy(d)];
+            if (cz(d) == 0) {
+                ld_dev2(p + z0, d, h[d].x, h[d].y);
+            } else if (cz(d) == 1) {
+                h[d] = ld_dev_pair(p + nb0.Z[0], p + z0, d);
+            } else {
+                h[d] = ld_dev_pair(p + z0 + 1, p + zp1, d);
+            }
+        }
+        bool fluid0 = true, fluid1 = true;
+        const bool face = on_walled_face(P, x, y, z0) || on_walled_face(P, x, y, z0 + 1);
+        if ((fl0 | fl1 | (int)face) != 0) {
+            fluid0 = resolve_state<M>(P, S, idx0, x, y, z0, fl0, nb0, Lane<0>{h});
+            Nbr nb1 = nb0;
+            nb1.Z[0] = z0;
+            nb1.Z[1] = z0 + 1;
+            nb1.Z[2] = zp1;
+            fluid1 = resolve_state<M>(P, S, idx0 + 1, x, y, z0 + 1, fl1, nb1, Lane<1>{h});
+        }
+        if constexpr (OUT != OUT_NONE) {
+            float f[Q];
+#pragma unroll
+            for (int d = 0; d < Q; ++d) f[d] = h[d].x;
+            emit<M, FM, OUT>(P, out, idx0, !fluid0, f, cons);
+#pragma unroll
+            for (int d = 0; d < Q; ++d) f[d] = h[d].y;
+            emit<M, FM, OUT>(P, out, idx0 + 1, !fluid1, f, cons);
+        }
+        M::template collide2<FM>(P, idx0, h, [&](int d, float2 v) {
+            st_dev2(S.dst[d] + idx0, d, fluid0 ? v.x : M::solid(P, d), fluid1 ? v.y : M::solid(P, d));
+        });
     }
     if constexpr ((OUT & OUT_SUMS) != 0) block_sum5(cons, out.partials);
 }

@@ -22,7 +22,9 @@ struct LaunchArgs {
     void* u;
     double* partials;   // optional per-block conservation partials (grid x 5)
     int block;
+    int vec;            // cells per thread of KERNEL_STEP (1, or 2 for ModeFast with nz even)
     cudaStream_t stream;
+    int* grid_used;     // optional: receives the launched grid size
 };
 
 // Output selection of a step launch (OUT_* bits of lbm_kernels.cuh) from the

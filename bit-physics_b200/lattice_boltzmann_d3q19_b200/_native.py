@@ -54,6 +54,8 @@ class LbmDesc(C.Structure):
         ("inflow_u", C.c_double * 3),
         ("device", C.c_int32),
         ("block_size", C.c_int32),
+        ("cells_per_thread", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 

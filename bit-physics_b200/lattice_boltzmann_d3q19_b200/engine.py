@@ -55,6 +55,7 @@ class Lattice:
         inflow_u=(0.0, 0.0, 0.0),
         device: int = 0,
         block_size: int = 0,
+        cells_per_thread: int = 0,
     ):
         nx, ny, nz = (int(s) for s in shape)
         if storage not in N.STORAGE:
@@ -82,6 +83,7 @@ class Lattice:
         d.inflow_rho = float(inflow_rho)
         d.device = int(device)
         d.block_size = int(block_size)
+        d.cells_per_thread = int(cells_per_thread)
         self.desc = d
         h = C.c_void_p()
         N.check(N.lib().lbm_create(C.byref(d), C.byref(h)))

@@ -83,6 +83,9 @@ typedef struct lbm_desc {
     double inflow_u[3];  /* inflow cell velocity                             */
     int32_t device;      /* CUDA device ordinal                              */
     int32_t block_size;  /* threads per block for the step kernels; 0 = auto */
+    int32_t cells_per_thread; /* step kernel: 1, or 2 (f32/f16/bf16 storage with
+                                 nz even); 0 = auto                          */
+    int32_t reserved;
 } lbm_desc;
 
 typedef struct lbm_lattice lbm_lattice;

@@ -166,6 +166,44 @@ def test_fast_storages_channel_and_drag(storage):
 
 
 @pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
+def test_two_cells_per_thread_matches_one(storage):
+    """k_step2 (two z-adjacent cells per thread) against k_step on the sphere
+    channel and on a walled box with an odd-sized x/y and even nz."""
+    for case in ("channel", "box"):
+        outs = []
+        for cpt in (1, 2):
+            if case == "channel":
+                flags, _ = __import__("lattice_boltzmann_d3q19_b200").geometry.sphere_channel(
+                    (40, 16, 14), n_spheres=4, radius=(2.0, 4.0), seed=5)
+                lat = Lattice((40, 16, 14), 0.56, storage=storage, inflow_u=(0.04, 0.0, 0.0), cells_per_thread=cpt)
+                lat.set_flags(flags)
+                f0 = random_state((40, 16, 14), 26, amp=0.01)
+            else:
+                lat = Lattice((7, 5, 10), 0.6, storage=storage, periodic=(False, False, False),
+                              wall_velocity={"y+": (0.05, 0.0, 0.0)}, cells_per_thread=cpt)
+                f0 = random_state((7, 5, 10), 27, amp=0.01)
+            with lat:
+                lat.set_populations(f0)
+                lat.step(20)
+                sums = lat.step_monitor(3)
+                outs.append((lat.get_populations(), sums))
+        diff = float(np.max(np.abs(outs[0][0] - outs[1][0])))
+        print(f"{case} {storage}: max |f(1 cell) - f(2 cells)| = {diff:.3e}")
+        assert diff <= FAST_TOL[storage]
+        # FP64 sums of per-cell values that each differ by at most ~diff
+        cells = outs[0][0][0].size
+        assert np.allclose(outs[0][1], outs[1][1], rtol=0.0, atol=4 * cells * FAST_TOL[storage])
+
+
+def test_two_cells_per_thread_rejected_where_unsupported():
+    with pytest.raises(LbmError) as e:
+        Lattice((4, 4, 5), 0.7, storage="f16", cells_per_thread=2)
+    assert e.value.code == N.LBM_ERR_UNSUPPORTED
+    with pytest.raises(LbmError):
+        Lattice((4, 4, 4), 0.7, storage="f64", cells_per_thread=2)
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
 def test_fast_storage_run_to_run_identical(storage):
     (gpu, _), _ = channel_case(storage=storage)
     f0 = random_state(gpu.shape, 24, amp=0.01)
