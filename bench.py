@@ -165,13 +165,14 @@ def channel_geometry():
 
 
 CELLS_PER_THREAD = 0  # 0: the library's choice
+STAGING = "auto"
 
 
 def make_lattice(storage: str, flags, device: int):
     from lattice_boltzmann_d3q19_b200 import Lattice
 
     lat = Lattice(SHAPE, TAU, storage=storage, inflow_u=(INFLOW_U, 0.0, 0.0), device=device,
-                  cells_per_thread=CELLS_PER_THREAD)
+                  cells_per_thread=CELLS_PER_THREAD, staging=STAGING)
     lat.set_flags(flags)
     lat.set_equilibrium(1.0, (INFLOW_U, 0.0, 0.0))
     return lat
@@ -355,7 +356,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         from lattice_boltzmann_d3q19_b200 import Lattice
 
         lat = Lattice(SHAPE, TAU, storage=args.storage, inflow_u=(INFLOW_U, 0.0, 0.0), device=dev,
-                      cells_per_thread=CELLS_PER_THREAD)
+                      cells_per_thread=CELLS_PER_THREAD, staging=STAGING)
         lat.set_populations(f0_pinned)  # allocate staging outside the timed region
         torch.cuda.synchronize()
         if dist_on:
@@ -440,9 +441,11 @@ def main():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cells-per-thread", type=int, default=0, choices=[0, 1, 2])
+    ap.add_argument("--staging", default="auto", choices=["auto", "registers", "tma"])
     args = ap.parse_args()
-    global CELLS_PER_THREAD
+    global CELLS_PER_THREAD, STAGING
     CELLS_PER_THREAD = args.cells_per_thread
+    STAGING = args.staging
     if args.warmup < 3 and args.impl == "ours":
         ap.error("--warmup must be >= 3")
     rank = int(os.environ.get("RANK", "0"))

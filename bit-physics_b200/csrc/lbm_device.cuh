@@ -82,6 +82,7 @@ struct Params {
     unsigned walled[3]; // 1 where the axis is not periodic
     int has_flags;
     int wall_sum_pairwise; // nx * nz == 1 (see ModeExact::rho_wall)
+    int* err;              // device error word (pipeline wait timeouts), may be null
     const uint8_t* flags;
     const uint32_t* bbmask; // (n): bit d set when the pull source of d is solid
     const void* force; // (3, n): double for ModeExact, float for ModeFast
@@ -146,6 +147,24 @@ __device__ __forceinline__ void st_dev2(__nv_bfloat16* p, int, float a, float b)
 {
     *reinterpret_cast<__nv_bfloat162*>(p) = __floats2bfloat162_rn(a, b);
 }
+// Shared-memory reads of staged populations, as deviations.
+__device__ __forceinline__ float ld_dev_sm(const float* p, int d) { return *p - wf(d); }
+__device__ __forceinline__ float ld_dev_sm(const __half* p, int) { return __half2float(*p); }
+__device__ __forceinline__ float ld_dev_sm(const __nv_bfloat16* p, int) { return __bfloat162float(*p); }
+__device__ __forceinline__ float2 ld_dev2_sm(const float* p, int d)
+{
+    const float2 v = *reinterpret_cast<const float2*>(p);
+    return make_float2(v.x - wf(d), v.y - wf(d));
+}
+__device__ __forceinline__ float2 ld_dev2_sm(const __half* p, int)
+{
+    return __half22float2(*reinterpret_cast<const __half2*>(p));
+}
+__device__ __forceinline__ float2 ld_dev2_sm(const __nv_bfloat16* p, int)
+{
+    return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
+}
+
 // Packed two-lane f32 arithmetic (sm_100 FFMA2 / FADD2 / FMUL2): lane x is
 // cell z, lane y cell z + 1.  Every operation is correctly rounded per lane.
 __device__ __forceinline__ float2 bc2(float s) { return make_float2(s, s); }

@@ -19,6 +19,15 @@
 
 namespace lbm {
 
+// Tile plan of the TMA-staged step kernel (lbm_tma.cuh).
+struct TileCfg {
+    int rows;        // y-rows per tile
+    int tiles_y;     // ceil(ny / rows)
+    int ntiles;      // nx * tiles_y
+    int stages;      // pipeline depth; 0 = the TMA path does not apply
+    int stage_elems; // 19 * rows * nz
+};
+
 // What a kernel writes besides the populations (template parameter OUT).
 enum OutBits : int { OUT_NONE = 0, OUT_RHO_U = 1, OUT_SUMS = 2 };
 

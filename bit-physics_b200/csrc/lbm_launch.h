@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "lbm_device.cuh"
+#include "lbm_kernels.cuh"
 
 namespace lbm {
 
@@ -25,6 +26,8 @@ struct LaunchArgs {
     int vec;            // cells per thread of KERNEL_STEP (1, or 2 for ModeFast with nz even)
     cudaStream_t stream;
     int* grid_used;     // optional: receives the launched grid size
+    int tma_grid;       // > 0: KERNEL_STEP runs the TMA-staged kernel with this grid
+    TileCfg tile;
 };
 
 // Output selection of a step launch (OUT_* bits of lbm_kernels.cuh) from the
@@ -42,6 +45,11 @@ cudaError_t launch_feq_init(int storage, const Params& P, const double* rho, con
                             cudaStream_t s);
 cudaError_t launch_mark_near_solid(const Params& P, uint8_t* flags, uint32_t* bbmask, cudaStream_t s);
 cudaError_t launch_reduce_partials(const double* partials, int nblocks, double* out5, cudaStream_t s);
+
+// TMA-staged step (lbm_tma.cu): tile plan for a lattice (stages == 0 when the
+// path does not apply) and the launch.
+TileCfg plan_tma(int storage, int nx, int ny, int nz, int* grid, int device);
+cudaError_t launch_tma_step(int storage, int force_mode, const LaunchArgs& a);
 
 // Record the calling thread's error message (lbm_last_error) and return code.
 int set_error(int code, const char* message);

@@ -27,6 +27,7 @@ LBM_ERR_NO_DEVICE = -7
 STORAGE = {"f64": 0, "f32": 1, "f16": 2, "bf16": 3}
 FORCE = {"none": 0, "uniform": 1, "field": 2, "drag": 3}
 FACES = {"x-": 0, "x+": 1, "y-": 2, "y+": 3, "z-": 4, "z+": 5}
+STAGING = {"auto": 0, "registers": 1, "tma": 2}
 CELL_FLUID, CELL_SOLID, CELL_INFLOW, CELL_OUTFLOW = 0, 1, 2, 3
 
 
@@ -55,7 +56,7 @@ class LbmDesc(C.Structure):
         ("device", C.c_int32),
         ("block_size", C.c_int32),
         ("cells_per_thread", C.c_int32),
-        ("reserved", C.c_int32),
+        ("staging", C.c_int32),
     ]
 
 

@@ -15,7 +15,10 @@ Beyond the reference (project semantics, pinned to the CPU oracle):
 * ``force_mode``: none / uniform body force / per-cell field / porosity
   drag F = body_force - beta(alpha) m with beta = k alpha / (1 + k alpha / 2);
 * ``storage``: f64 (reference order), f32, or 16-bit deviations from the
-  weights (f16 / bf16, "shift" storage) with f32 arithmetic.
+  weights (f16 / bf16, "shift" storage) with f32 arithmetic;
+* ``staging`` / ``cells_per_thread``: which step kernel runs (register-
+  staged one or two cells per thread, or TMA shared-memory staging); they
+  change speed, not semantics.
 """
 
 from __future__ import annotations
@@ -56,6 +59,7 @@ class Lattice:
         device: int = 0,
         block_size: int = 0,
         cells_per_thread: int = 0,
+        staging: str = "auto",
     ):
         nx, ny, nz = (int(s) for s in shape)
         if storage not in N.STORAGE:
@@ -84,6 +88,9 @@ class Lattice:
         d.device = int(device)
         d.block_size = int(block_size)
         d.cells_per_thread = int(cells_per_thread)
+        if staging not in N.STAGING:
+            raise ValueError(f"staging must be one of {sorted(N.STAGING)}")
+        d.staging = N.STAGING[staging]
         self.desc = d
         h = C.c_void_p()
         N.check(N.lib().lbm_create(C.byref(d), C.byref(h)))

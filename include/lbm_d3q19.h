@@ -85,8 +85,15 @@ typedef struct lbm_desc {
     int32_t block_size;  /* threads per block for the step kernels; 0 = auto */
     int32_t cells_per_thread; /* step kernel: 1, or 2 (f32/f16/bf16 storage with
                                  nz even); 0 = auto                          */
-    int32_t reserved;
+    int32_t staging;     /* step kernel input staging: LBM_STAGING_*         */
 } lbm_desc;
+
+/* Step-kernel staging (lbm_desc.staging). */
+#define LBM_STAGING_AUTO 0      /* the fastest measured: registers               */
+#define LBM_STAGING_REGISTERS 1 /* loads straight into registers                  */
+#define LBM_STAGING_TMA 2       /* TMA bulk copies into a shared-memory ring: two
+                                   cells per thread, f32/f16/bf16 storage, nz even
+                                   and nz * element size a multiple of 16 bytes   */
 
 typedef struct lbm_lattice lbm_lattice;
 

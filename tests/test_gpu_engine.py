@@ -195,6 +195,64 @@ def test_two_cells_per_thread_matches_one(storage):
         assert np.allclose(outs[0][1], outs[1][1], rtol=0.0, atol=4 * cells * FAST_TOL[storage])
 
 
+TMA_CASES = [
+    # shape, tau, periodic, walls, with flags: rows per tile 8 with a partial
+    # last tile (ny = 9 / 10), y walls (wrap splits of the row copies), flags
+    ((12, 9, 16), 0.6, (True, False, True), {"y+": (0.04, 0.0, 0.0), "y-": (0.0, 0.0, -0.01)}, False),
+    ((10, 10, 32), 0.56, (True, True, True), None, True),
+    ((6, 3, 8), 0.7, (False, True, False), {"x-": (0.0, 0.02, 0.0), "z+": (0.01, 0.0, 0.0)}, True),
+]
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
+@pytest.mark.parametrize("case", range(len(TMA_CASES)))
+def test_tma_staging_matches_oracle_and_registers(storage, case):
+    """The TMA-staged kernel against the CPU oracle (same storage rounding)
+    and against the register-staged two-cell kernel."""
+    shape, tau, periodic, walls, with_flags = TMA_CASES[case]
+    if storage == "f32" and (shape[2] * 4) % 16:
+        pytest.skip("row not a multiple of 16 bytes")
+    flags = None
+    if with_flags:
+        flags = np.zeros(shape, dtype=np.uint8)
+        flags[0] = 2
+        flags[-1] = 3
+        flags[shape[0] // 2, 1:3, 2:5] = 1
+    f0 = random_state(shape, 40 + case, amp=0.01)
+    outs = {}
+    for staging in ("tma", "registers"):
+        gpu, cpu = pair(shape, tau, storage, periodic=periodic, wall_velocity=walls, flags=flags,
+                        inflow_u=(0.03, 0.0, 0.0))
+        gpu.close()
+        lat = Lattice(shape, tau, storage=storage, periodic=periodic, wall_velocity=walls,
+                      inflow_u=(0.03, 0.0, 0.0), staging=staging, cells_per_thread=2)
+        with lat:
+            if flags is not None:
+                lat.set_flags(flags)
+            lat.set_populations(f0)
+            lat.step(1)
+            lat.step(15)
+            sums = lat.step_monitor(4)
+            outs[staging] = (lat.get_populations(), sums, lat.rho_u())
+        cpu.set_populations(f0)
+        cpu.step(20)
+    fc = cpu.get_populations()
+    d_oracle = float(np.max(np.abs(outs["tma"][0] - fc)))
+    d_regs = float(np.max(np.abs(outs["tma"][0] - outs["registers"][0])))
+    print(f"case {case} {storage}: tma vs oracle {d_oracle:.3e}, tma vs registers {d_regs:.3e}")
+    assert d_oracle <= FAST_TOL[storage] and d_regs <= FAST_TOL[storage]
+    cells = fc[0].size
+    assert np.allclose(outs["tma"][1], outs["registers"][1], rtol=0.0, atol=4 * cells * FAST_TOL[storage])
+
+
+def test_tma_staging_rejected_where_unsupported():
+    with pytest.raises(LbmError) as e:
+        Lattice((4, 4, 6), 0.7, storage="f16", staging="tma")   # 12-byte rows
+    assert e.value.code == N.LBM_ERR_UNSUPPORTED
+    with pytest.raises(LbmError):
+        Lattice((4, 4, 8), 0.7, storage="f64", staging="tma")
+
+
 def test_two_cells_per_thread_rejected_where_unsupported():
     with pytest.raises(LbmError) as e:
         Lattice((4, 4, 5), 0.7, storage="f16", cells_per_thread=2)
