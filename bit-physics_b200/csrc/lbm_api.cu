@@ -951,3 +951,359 @@ int lbm_bounce_back_y_walls(const double* f, double* f_out, int32_t nx, int32_t 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batches
+// ---------------------------------------------------------------------------
+#include "lbm_batch.cuh"
+
+struct lbm_batch {
+    int count = 0;
+    int storage = 0;
+    int force_mode = 0;
+    int device = 0;
+    std::vector<lbm_lattice*> lats;
+    cudaStream_t stream = nullptr;
+    void* records = nullptr;       // count BatchLattice records (layout independent of T)
+    std::vector<BatchLattice<float>> host_records;
+    BatchItem* items = nullptr;
+    int nitems = 0;
+    int items_cap = 0;
+    int sched = SCHED_SINGLE;
+    int block = 256;
+    int grid = 0;
+    int sms = 1;
+    cudaGraphExec_t graph = nullptr;
+    bool graph_valid = false;
+};
+
+namespace {
+
+int batch_span(const lbm_batch* b) { return b->block * (b->sched == SCHED_SINGLE ? 1 : 2); }
+
+int batch_build_items(lbm_batch* b)
+{
+    const int span = batch_span(b);
+    std::vector<BatchItem> items;
+    for (int i = 0; i < b->count; ++i)
+        for (int c = 0; c < b->lats[i]->n; c += span) items.push_back(BatchItem{i, c});
+    if ((int)items.size() > b->items_cap) {
+        if (b->items) CK(cudaFree(b->items), "batch items free");
+        b->items = nullptr;
+        b->items_cap = 0;
+        CK(cudaMalloc((void**)&b->items, sizeof(BatchItem) * items.size()), "batch items allocation");
+        b->items_cap = (int)items.size();
+    }
+    CK(cudaMemcpy(b->items, items.data(), sizeof(BatchItem) * items.size(), cudaMemcpyHostToDevice), "items upload");
+    b->nitems = (int)items.size();
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    b->graph_valid = false;
+    return LBM_OK;
+}
+
+int batch_grid(const lbm_batch* b)
+{
+    const int g = b->grid > 0 ? b->grid : 4 * b->sms;
+    return g < b->nitems ? g : b->nitems;
+}
+
+// Records for the next steps: phase 0 reads buf[cur], phase 1 the other.
+int batch_upload_records(lbm_batch* b)
+{
+    for (int i = 0; i < b->count; ++i) {
+        lbm_lattice* h = b->lats[i];
+        BatchLattice<float>& r = b->host_records[i];
+        r.P = h->P;
+        r.S[0] = make_streams<float>(nullptr, nullptr, h->n);
+        // the pointer layout does not depend on T: fill as bytes of the storage
+        for (int d = 0; d < Q; ++d) {
+            const char* a = (const char*)h->buf[h->cur] + (size_t)d * h->n * h->elem;
+            const char* c = (const char*)h->buf[h->cur ^ 1] + (size_t)d * h->n * h->elem;
+            r.S[0].src[d] = (const float*)a;
+            r.S[0].dst[d] = (float*)c;
+            r.S[1].src[d] = (const float*)c;
+            r.S[1].dst[d] = (float*)a;
+        }
+        r.vec = (h->storage != LBM_STORAGE_F64 && h->desc.nz % 2 == 0) ? 2 : 1;
+    }
+    CK(cudaMemcpyAsync(b->records, b->host_records.data(), sizeof(BatchLattice<float>) * b->count,
+                       cudaMemcpyHostToDevice, b->stream),
+       "records upload");
+    return LBM_OK;
+}
+
+void batch_advance_bookkeeping(lbm_batch* b, int steps)
+{
+    for (lbm_lattice* h : b->lats) {
+        if (steps % 2) h->cur ^= 1;
+        h->pre = false;
+        h->steps += steps;
+    }
+}
+
+cudaError_t batch_launch(lbm_batch* b, bool collide, int phase)
+{
+    return launch_batch_step(b->storage, b->force_mode, b->sched, collide, b->records, b->items, b->nitems,
+                             batch_span(b), phase, batch_grid(b), b->block, b->stream);
+}
+
+int batch_check(lbm_batch* b)
+{
+    if (!b) return fail(LBM_ERR_INVALID, "null batch handle");
+    CK(cudaSetDevice(b->device), "cudaSetDevice");
+    for (lbm_lattice* h : b->lats) {
+        int rc = check_force_ready(h);
+        if (rc) return rc;
+    }
+    return LBM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_batch_create(const lbm_desc* descs, int32_t count, lbm_batch** out)
+{
+    if (!descs || !out || count < 1) return fail(LBM_ERR_INVALID, "need descriptors, count >= 1 and an output");
+    *out = nullptr;
+    for (int i = 1; i < count; ++i)
+        if (descs[i].storage != descs[0].storage || descs[i].force_mode != descs[0].force_mode ||
+            descs[i].device != descs[0].device)
+            return fail(LBM_ERR_INVALID, "lattices of a batch share storage, force model and device");
+    lbm_batch* b = new lbm_batch();
+    b->count = count;
+    b->storage = descs[0].storage;
+    b->force_mode = descs[0].force_mode;
+    b->device = descs[0].device;
+    auto cleanup = [&](int code) {
+        lbm_batch_destroy(b);
+        return code;
+    };
+    int rc;
+    for (int i = 0; i < count; ++i) {
+        lbm_lattice* h = nullptr;
+        if ((rc = lbm_create(&descs[i], &h))) return cleanup(rc);
+        b->lats.push_back(h);
+    }
+    cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "batch stream"));
+    for (lbm_lattice* h : b->lats)
+        if ((rc = lbm_set_stream(h, b->stream))) return cleanup(rc);
+    b->host_records.resize(count);
+    e = cudaMalloc(&b->records, sizeof(BatchLattice<float>) * count);
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "batch records"));
+    cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device);
+    if (b->sms < 1) b->sms = 1;
+    if ((rc = batch_build_items(b))) return cleanup(rc);
+    *out = b;
+    return LBM_OK;
+}
+
+int lbm_batch_destroy(lbm_batch* b)
+{
+    if (!b) return LBM_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    for (lbm_lattice* h : b->lats) {
+        h->stream = nullptr;  // the batch owns the stream
+        h->own_stream = false;
+        lbm_destroy(h);
+    }
+    if (b->records) cudaFree(b->records);
+    if (b->items) cudaFree(b->items);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return LBM_OK;
+}
+
+int lbm_batch_count(const lbm_batch* b) { return b ? b->count : -1; }
+
+int lbm_batch_lattice(lbm_batch* b, int32_t i, lbm_lattice** out)
+{
+    if (!b || !out || i < 0 || i >= b->count) return fail(LBM_ERR_INVALID, "bad batch index");
+    *out = b->lats[i];
+    return LBM_OK;
+}
+
+int lbm_batch_set_schedule(lbm_batch* b, int32_t sched, int32_t block, int32_t grid)
+{
+    if (!b) return fail(LBM_ERR_INVALID, "null batch handle");
+    if (sched < SCHED_SINGLE || sched > SCHED_PAIR_MIXED) return fail(LBM_ERR_INVALID, "unknown schedule %d", sched);
+    if (sched != SCHED_SINGLE && (b->storage == LBM_STORAGE_F64 || b->force_mode == LBM_FORCE_FIELD ||
+                                  b->force_mode == LBM_FORCE_DRAG))
+        return fail(LBM_ERR_UNSUPPORTED, "two-cell schedules need f32/f16/bf16 storage and no per-cell force");
+    if (block < 32 || block > 256 || block % 32) return fail(LBM_ERR_INVALID, "block must be a multiple of 32 <= 256");
+    if (grid < 0) return fail(LBM_ERR_INVALID, "negative grid");
+    CK(cudaSetDevice(b->device), "cudaSetDevice");
+    b->sched = sched;
+    b->block = block;
+    b->grid = grid;
+    return batch_build_items(b);
+}
+
+int lbm_batch_get_schedule(const lbm_batch* b, int32_t* sched, int32_t* block, int32_t* grid)
+{
+    if (!b) return fail(LBM_ERR_INVALID, "null batch handle");
+    if (sched) *sched = b->sched;
+    if (block) *block = b->block;
+    if (grid) *grid = batch_grid(b);
+    return LBM_OK;
+}
+
+int lbm_batch_synchronize(lbm_batch* b)
+{
+    if (!b) return fail(LBM_ERR_INVALID, "null batch handle");
+    CK(cudaSetDevice(b->device), "cudaSetDevice");
+    CK(cudaStreamSynchronize(b->stream), "batch sync");
+    return LBM_OK;
+}
+
+int lbm_batch_step(lbm_batch* b, int32_t n_steps)
+{
+    int rc = batch_check(b);
+    if (rc) return rc;
+    if (n_steps < 0) return fail(LBM_ERR_INVALID, "negative step count");
+    int done = 0;
+    // First step: lattices holding f_n collide in place.  A batch whose
+    // lattices are in different states takes one step lattice by lattice.
+    int n_pre = 0;
+    for (lbm_lattice* h : b->lats) n_pre += h->pre ? 1 : 0;
+    if (n_steps > 0 && n_pre > 0) {
+        if (n_pre == b->count) {
+            if ((rc = batch_upload_records(b))) return rc;
+            CK(batch_launch(b, true, 0), "batch collide launch");
+            batch_advance_bookkeeping(b, 1);
+        } else {
+            for (lbm_lattice* h : b->lats)
+                if ((rc = advance(h, nullptr, nullptr, nullptr))) return rc;
+        }
+        done = 1;
+    }
+    const int rest = n_steps - done;
+    if (rest <= 0) return LBM_OK;
+    if ((rc = batch_upload_records(b))) return rc;
+    if (rest >= 2 && !b->graph_valid) {
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "graph capture begin");
+        cudaError_t e0 = batch_launch(b, false, 0);
+        cudaError_t e1 = batch_launch(b, false, 1);
+        cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+        if (e0 != cudaSuccess || e1 != cudaSuccess || e2 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return cuda_fail(e0 != cudaSuccess ? e0 : (e1 != cudaSuccess ? e1 : e2), "batch graph capture");
+        }
+        cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return cuda_fail(e, "batch graph instantiate");
+        b->graph_valid = true;
+    }
+    for (int k = 0; k + 1 < rest; k += 2) CK(cudaGraphLaunch(b->graph, b->stream), "batch graph launch");
+    if (rest % 2) CK(batch_launch(b, false, 0), "batch step launch");
+    batch_advance_bookkeeping(b, rest);
+    return LBM_OK;
+}
+
+int lbm_batch_step_unbatched(lbm_batch* b, int32_t n_steps)
+{
+    int rc = batch_check(b);
+    if (rc) return rc;
+    if (n_steps < 0) return fail(LBM_ERR_INVALID, "negative step count");
+    for (int s = 0; s < n_steps; ++s)
+        for (lbm_lattice* h : b->lats)
+            if ((rc = advance(h, nullptr, nullptr, nullptr))) return rc;
+    return LBM_OK;
+}
+
+int lbm_batch_autotune(lbm_batch* b, int32_t trial_steps, double* best_ms)
+{
+    int rc = batch_check(b);
+    if (rc) return rc;
+    if (trial_steps < 2) return fail(LBM_ERR_INVALID, "trial_steps must be >= 2");
+    trial_steps += trial_steps % 2;  // even: every lattice returns to its buffer parity
+    // Save both buffers and the state flags of every lattice.
+    std::vector<void*> saved;
+    for (lbm_lattice* h : b->lats) {
+        const size_t bytes = h->elem * Q * (size_t)h->n;
+        for (int k = 0; k < 2; ++k) {
+            void* p = nullptr;
+            cudaError_t e = cudaMalloc(&p, bytes);
+            if (e != cudaSuccess) {
+                for (void* q : saved) cudaFree(q);
+                return cuda_fail(e, "autotune snapshot");
+            }
+            cudaMemcpyAsync(p, h->buf[k], bytes, cudaMemcpyDeviceToDevice, b->stream);
+            saved.push_back(p);
+        }
+    }
+    std::vector<int> cur0, pre0;
+    std::vector<int64_t> steps0;
+    for (lbm_lattice* h : b->lats) {
+        cur0.push_back(h->cur);
+        pre0.push_back(h->pre);
+        steps0.push_back(h->steps);
+    }
+    const int old_sched = b->sched, old_block = b->block, old_grid = b->grid;
+    // warm the lattices into the steady state once
+    if ((rc = lbm_batch_step(b, 1))) goto restore;
+    {
+        std::vector<int> scheds = {SCHED_SINGLE};
+        if (b->storage != LBM_STORAGE_F64 && (b->force_mode == LBM_FORCE_NONE || b->force_mode == LBM_FORCE_UNIFORM)) {
+            scheds.push_back(SCHED_PAIR_SCALAR);
+            scheds.push_back(SCHED_PAIR_MIXED);
+        }
+        double best = 1e30;
+        int bs = old_sched, bb = old_block, bg = old_grid;
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        for (int sc : scheds)
+            for (int blk : {128, 256})
+                for (int per_sm : {2, 4, 8}) {
+                    if ((rc = lbm_batch_set_schedule(b, sc, blk, per_sm * b->sms))) break;
+                    if ((rc = lbm_batch_step(b, 2))) break;  // capture + warm
+                    cudaEventRecord(e0, b->stream);
+                    if ((rc = lbm_batch_step(b, trial_steps))) break;
+                    cudaEventRecord(e1, b->stream);
+                    cudaEventSynchronize(e1);
+                    float ms = 0.0f;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    const double per = ms / trial_steps;
+                    if (per < best) {
+                        best = per;
+                        bs = sc;
+                        bb = blk;
+                        bg = per_sm * b->sms;
+                    }
+                }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (rc == LBM_OK) {
+            if (best_ms) *best_ms = best;
+            rc = lbm_batch_set_schedule(b, bs, bb, bg);
+            goto restore_state;
+        }
+    }
+restore:
+    lbm_batch_set_schedule(b, old_sched, old_block, old_grid);
+restore_state:
+    cudaStreamSynchronize(b->stream);
+    for (int i = 0; i < b->count; ++i) {
+        lbm_lattice* h = b->lats[i];
+        const size_t bytes = h->elem * Q * (size_t)h->n;
+        for (int k = 0; k < 2; ++k) {
+            cudaMemcpyAsync(h->buf[k], saved[2 * i + k], bytes, cudaMemcpyDeviceToDevice, b->stream);
+        }
+        h->cur = cur0[i];
+        h->pre = pre0[i];
+        h->steps = steps0[i];
+    }
+    cudaStreamSynchronize(b->stream);
+    for (void* p : saved) cudaFree(p);
+    return rc;
+}
+
+}  // extern "C"

@@ -7,6 +7,7 @@
 //                                                is rounded once, as the CPU
 //                                                oracle's store_round does)
 //   the stateless reference functions           (d3q19_warp.py:87-212, :253-415)
+#include "lbm_batch.cuh"
 #include "lbm_kernels.cuh"
 #include "lbm_launch.h"
 
@@ -57,6 +58,34 @@ cudaError_t launch_exact(int kernel, int force_mode, const LaunchArgs& a)
     case FORCE_UNIFORM: return launch_exact_fm<FORCE_UNIFORM>(kernel, a);
     case FORCE_FIELD: return launch_exact_fm<FORCE_FIELD>(kernel, a);
     case FORCE_DRAG: return launch_exact_fm<FORCE_DRAG>(kernel, a);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+// Batched step, f64 storage (one cell per thread).
+template <int FM>
+static cudaError_t batch_exact_fm(bool collide, const void* records, const void* items, int nitems, int span,
+                                  int phase, int grid, int block, cudaStream_t s)
+{
+    using M = ModeExact;
+    const auto* L = (const BatchLattice<double>*)records;
+    const auto* I = (const BatchItem*)items;
+    if (collide)
+        k_collide_batch<M, FM><<<grid, block, 0, s>>>(L, I, nitems, span, phase);
+    else
+        k_step_batch<M, FM, SCHED_SINGLE><<<grid, block, 0, s>>>(L, I, nitems, phase);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_exact(int force_mode, bool collide, const void* records, const void* items, int nitems,
+                               int span, int phase, int grid, int block, cudaStream_t s)
+{
+    switch (force_mode) {
+    case FORCE_NONE: return batch_exact_fm<FORCE_NONE>(collide, records, items, nitems, span, phase, grid, block, s);
+    case FORCE_UNIFORM:
+        return batch_exact_fm<FORCE_UNIFORM>(collide, records, items, nitems, span, phase, grid, block, s);
+    case FORCE_FIELD: return batch_exact_fm<FORCE_FIELD>(collide, records, items, nitems, span, phase, grid, block, s);
+    case FORCE_DRAG: return batch_exact_fm<FORCE_DRAG>(collide, records, items, nitems, span, phase, grid, block, s);
     default: return cudaErrorInvalidValue;
     }
 }

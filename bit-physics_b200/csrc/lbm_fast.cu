@@ -1,5 +1,6 @@
 // lbm_fast.cu -- f32-arithmetic step kernels for f32, binary16-shift and
 // bfloat16-shift storage (ModeFast).  Built with multiply-add contraction on.
+#include "lbm_batch.cuh"
 #include "lbm_kernels.cuh"
 #include "lbm_launch.h"
 
@@ -55,6 +56,80 @@ static cudaError_t launch_fast_fm(int kernel, int force_mode, const LaunchArgs& 
     case FORCE_FIELD: return launch_fast_t<T, FORCE_FIELD>(kernel, a);
     case FORCE_DRAG: return launch_fast_t<T, FORCE_DRAG>(kernel, a);
     default: return cudaErrorInvalidValue;
+    }
+}
+
+template <class T, int FM>
+static cudaError_t batch_fm(int sched, bool collide, const void* records, const void* items, int nitems, int span,
+                            int phase, int grid, int block, cudaStream_t s)
+{
+    using M = ModeFast<T>;
+    const auto* L = (const BatchLattice<T>*)records;
+    const auto* I = (const BatchItem*)items;
+    if (collide) {
+        k_collide_batch<M, FM><<<grid, block, 0, s>>>(L, I, nitems, span, phase);
+        return cudaGetLastError();
+    }
+    if constexpr (FM == FORCE_NONE || FM == FORCE_UNIFORM) {
+        if (sched == SCHED_PAIR_SCALAR) {
+            k_step_batch<M, FM, SCHED_PAIR_SCALAR><<<grid, block, 0, s>>>(L, I, nitems, phase);
+            return cudaGetLastError();
+        }
+        if (sched == SCHED_PAIR_MIXED) {
+            k_step_batch<M, FM, SCHED_PAIR_MIXED><<<grid, block, 0, s>>>(L, I, nitems, phase);
+            return cudaGetLastError();
+        }
+    }
+    if (sched != SCHED_SINGLE) return cudaErrorInvalidValue;
+    k_step_batch<M, FM, SCHED_SINGLE><<<grid, block, 0, s>>>(L, I, nitems, phase);
+    return cudaGetLastError();
+}
+
+template <class T>
+static cudaError_t batch_t(int force_mode, int sched, bool collide, const void* records, const void* items,
+                           int nitems, int span, int phase, int grid, int block, cudaStream_t s)
+{
+    switch (force_mode) {
+    case FORCE_NONE: return batch_fm<T, FORCE_NONE>(sched, collide, records, items, nitems, span, phase, grid, block, s);
+    case FORCE_UNIFORM:
+        return batch_fm<T, FORCE_UNIFORM>(sched, collide, records, items, nitems, span, phase, grid, block, s);
+    case FORCE_FIELD:
+        return batch_fm<T, FORCE_FIELD>(sched, collide, records, items, nitems, span, phase, grid, block, s);
+    case FORCE_DRAG: return batch_fm<T, FORCE_DRAG>(sched, collide, records, items, nitems, span, phase, grid, block, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_batch_exact(int force_mode, bool collide, const void* records, const void* items, int nitems,
+                               int span, int phase, int grid, int block, cudaStream_t s);
+
+cudaError_t launch_batch_step(int storage, int force_mode, int sched, bool collide, const void* records,
+                              const void* items, int nitems, int span, int phase, int grid, int block,
+                              cudaStream_t s)
+{
+    switch (storage) {
+    case STORAGE_F64:
+        if (sched != SCHED_SINGLE && !collide) return cudaErrorInvalidValue;
+        return launch_batch_exact(force_mode, collide, records, items, nitems, span, phase, grid, block, s);
+    case STORAGE_F32:
+        return batch_t<float>(force_mode, sched, collide, records, items, nitems, span, phase, grid, block, s);
+    case STORAGE_F16:
+        return batch_t<__half>(force_mode, sched, collide, records, items, nitems, span, phase, grid, block, s);
+    case STORAGE_BF16:
+        return batch_t<__nv_bfloat16>(force_mode, sched, collide, records, items, nitems, span, phase, grid, block,
+                                      s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+size_t batch_record_bytes(int storage)
+{
+    switch (storage) {
+    case STORAGE_F64: return sizeof(BatchLattice<double>);
+    case STORAGE_F32: return sizeof(BatchLattice<float>);
+    case STORAGE_F16: return sizeof(BatchLattice<__half>);
+    case STORAGE_BF16: return sizeof(BatchLattice<__nv_bfloat16>);
+    default: return 0;
     }
 }
 

@@ -104,32 +104,37 @@ __device__ __forceinline__ void store_solid(const Params& P, const Streams<typen
     for (int d = 0; d < Q; ++d) M::store(S.dst[d] + idx, d, M::solid(P, d));
 }
 
-// Fused step from POST: f_n = gather + resolve_state(P_{n-1}); optional
-// outputs of f_n; P_n = collide(f_n).  Solid cells store their rest value.
-// The own-position gather is issued before the flag byte is examined, so the
-// 19 loads and the flag load are in flight together.
+// Fused step from POST for one cell: f_n = gather + resolve_state(P_{n-1});
+// optional outputs of f_n; P_n = collide(f_n).  Solid cells store their rest
+// value.  The own-position gather is issued before the flag byte is examined,
+// so the 19 loads and the flag load are in flight together.
+template <class M, int FM, int OUT>
+__device__ __forceinline__ void step_single(const Params& P, const Streams<typename M::T>& S,
+                                            const Outputs<typename M::C>& out, int idx, double* cons)
+{
+    using C = typename M::C;
+    int x, y, z;
+    decode_xyz(P, idx, x, y, z);
+    const int fl = P.has_flags ? (int)P.flags[idx] : 0;
+    const Nbr nb = make_nbr(P, x, y, z);
+    C f[Q];
+    gather<M>(S, nb, f);
+    if (resolve_state<M>(P, S, idx, x, y, z, fl, nb, f)) {
+        emit<M, FM, OUT>(P, out, idx, false, f, cons);
+        M::template collide<FM>(P, idx, f);
+        store_all<M>(S, idx, f);
+    } else {
+        emit<M, FM, OUT>(P, out, idx, true, f, cons);
+        store_solid<M>(P, S, idx);
+    }
+}
+
 template <class M, int FM, int OUT>
 __global__ void __launch_bounds__(256) k_step(Params P, Streams<typename M::T> S, Outputs<typename M::C> out)
 {
-    using C = typename M::C;
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     double cons[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    if (idx < P.n) {
-        int x, y, z;
-        decode_xyz(P, idx, x, y, z);
-        const int fl = P.has_flags ? (int)P.flags[idx] : 0;
-        const Nbr nb = make_nbr(P, x, y, z);
-        C f[Q];
-        gather<M>(S, nb, f);
-        if (resolve_state<M>(P, S, idx, x, y, z, fl, nb, f)) {
-            emit<M, FM, OUT>(P, out, idx, false, f, cons);
-            M::template collide<FM>(P, idx, f);
-            store_all<M>(S, idx, f);
-        } else {
-            emit<M, FM, OUT>(P, out, idx, true, f, cons);
-            store_solid<M>(P, S, idx);
-        }
-    }
+    if (idx < P.n) step_single<M, FM, OUT>(P, S, out, idx, cons);
     if constexpr ((OUT & OUT_SUMS) != 0) block_sum5(cons, out.partials);
 }
 
@@ -140,85 +145,129 @@ __global__ void __launch_bounds__(256) k_step(Params P, Streams<typename M::T> S
 // per operation for the two cells).  The 9 directions with c_z = 0 pull both
 // values with one vector load, the 10 z-shifted ones with two scalar loads;
 // all 19 stores are vector stores.  Cells that need a boundary rule are
-// resolved one at a time with k_step's scalar resolve_state.
+// resolved one at a time with the scalar resolve_state.
 template <class M, int FM, int OUT>
-__global__ void __launch_bounds__(256, LBM_STEP2_MIN_BLOCKS) k_step2(Params P, Streams<typename M::T> S, Outputs<typename M::C> out)
+__device__ __forceinline__ void step_pair(const Params& P, const Streams<typename M::T>& S,
+                                          const Outputs<typename M::C>& out, int idx0, double* cons)
 {
     using T = typename M::T;
+    int x, y, z0;
+    decode_xyz(P, idx0, x, y, z0);
+    int fl0 = 0, fl1 = 0;
+    if (P.has_flags) {
+        const unsigned short both = __ldg(reinterpret_cast<const unsigned short*>(P.flags + idx0));
+        fl0 = both & 0xff;
+        fl1 = both >> 8;
+    }
+    const Nbr nb0 = make_nbr(P, x, y, z0);
+    const int zp1 = z0 + 2 == P.nz ? 0 : z0 + 2; // (z0 + 1) + 1, wrapped
+    float2 h[Q];
+#pragma unroll
+    for (int d = 0; d < Q; ++d) {
+        const T* p = S.src[d] + nb0.X[1 - cx(d)] + nb0.Y[1 - cy(d)];
+        if (cz(d) == 0) {
+            ld_dev2(p + z0, d, h[d].x, h[d].y);
+        } else if (cz(d) == 1) {
+            h[d] = ld_dev_pair(p + nb0.Z[0], p + z0, d);
+        } else {
+            h[d] = ld_dev_pair(p + z0 + 1, p + zp1, d);
+        }
+    }
+    bool fluid0 = true, fluid1 = true;
+    const bool face = on_walled_face(P, x, y, z0) || on_walled_face(P, x, y, z0 + 1);
+    if ((fl0 | fl1 | (int)face) != 0) {
+        fluid0 = resolve_state<M>(P, S, idx0, x, y, z0, fl0, nb0, Lane<0>{h});
+        Nbr nb1 = nb0;
+        nb1.Z[0] = z0;
+        nb1.Z[1] = z0 + 1;
+        nb1.Z[2] = zp1;
+        fluid1 = resolve_state<M>(P, S, idx0 + 1, x, y, z0 + 1, fl1, nb1, Lane<1>{h});
+    }
+    if constexpr (OUT != OUT_NONE) {
+        float f[Q];
+#pragma unroll
+        for (int d = 0; d < Q; ++d) f[d] = h[d].x;
+        emit<M, FM, OUT>(P, out, idx0, !fluid0, f, cons);
+#pragma unroll
+        for (int d = 0; d < Q; ++d) f[d] = h[d].y;
+        emit<M, FM, OUT>(P, out, idx0 + 1, !fluid1, f, cons);
+    }
+    M::template collide2<FM>(P, idx0, h, [&](int d, float2 v) {
+        st_dev2(S.dst[d] + idx0, d, fluid0 ? v.x : M::solid(P, d), fluid1 ? v.y : M::solid(P, d));
+    });
+}
+
+// Two consecutive cells idx0, idx0 + 1 of any lattice (they may sit in
+// different rows, and idx0 + 1 may be past the end) with scalar memory
+// accesses and the packed f32x2 collision.  Used by the batched step for
+// lattices whose rows are not even-length.
+template <class M, int FM>
+__device__ __forceinline__ void step_pair_scalar(const Params& P, const Streams<typename M::T>& S, int idx0)
+{
+    const int idx1 = idx0 + 1 < P.n ? idx0 + 1 : idx0;  // a lone last cell is computed twice, stored once
+    int x0, y0, z0, x1, y1, z1;
+    decode_xyz(P, idx0, x0, y0, z0);
+    decode_xyz(P, idx1, x1, y1, z1);
+    const int fl0 = P.has_flags ? (int)P.flags[idx0] : 0;
+    const int fl1 = P.has_flags ? (int)P.flags[idx1] : 0;
+    const Nbr nb0 = make_nbr(P, x0, y0, z0);
+    const Nbr nb1 = make_nbr(P, x1, y1, z1);
+    float2 h[Q];
+#pragma unroll
+    for (int d = 0; d < Q; ++d) h[d] = ld_dev_pair(S.src[d] + nb0.src(d), S.src[d] + nb1.src(d), d);
+    bool fluid0 = true, fluid1 = true;
+    if ((fl0 | fl1 | (int)on_walled_face(P, x0, y0, z0) | (int)on_walled_face(P, x1, y1, z1)) != 0) {
+        fluid0 = resolve_state<M>(P, S, idx0, x0, y0, z0, fl0, nb0, Lane<0>{h});
+        fluid1 = resolve_state<M>(P, S, idx1, x1, y1, z1, fl1, nb1, Lane<1>{h});
+    }
+    const bool two = idx1 != idx0;
+    // The packed collision reads (cell, cell + 1) pairs of per-cell force
+    // inputs; the scalar path serves the force-free and uniform models only.
+    static_assert(FM == FORCE_NONE || FM == FORCE_UNIFORM, "step_pair_scalar: per-cell forces unsupported");
+    M::template collide2<FM>(P, idx0, h, [&](int d, float2 v) {
+        M::store(S.dst[d] + idx0, d, fluid0 ? v.x : M::solid(P, d));
+        if (two) M::store(S.dst[d] + idx1, d, fluid1 ? v.y : M::solid(P, d));
+    });
+}
+
+template <class M, int FM, int OUT>
+__global__ void __launch_bounds__(256, LBM_STEP2_MIN_BLOCKS) k_step2(Params P, Streams<typename M::T> S,
+                                                                    Outputs<typename M::C> out)
+{
     const int idx0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
     double cons[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    if (idx0 < P.n) {
-        int x, y, z0;
-        decode_xyz(P, idx0, x, y, z0);
-        int fl0 = 0, fl1 = 0;
-        if (P.has_flags) {
-            const unsigned short both = __ldg(reinterpret_cast<const unsigned short*>(P.flags + idx0));
-            fl0 = both & 0xff;
-            fl1 = both >> 8;
-        }
-        const Nbr nb0 = make_nbr(P, x, y, z0);
-        const int zp1 = z0 + 2 == P.nz ? 0 : z0 + 2; // (z0 + 1) + 1, wrapped
-        float2 h[Q];
-#pragma unroll
-        for (int d = 0; d < Q; ++d) {
-            const T* p = S.src[d] + nb0.X[1 - cx(d)] + nb0.Y[1 - cy(d)];
-            if (cz(d) == 0) {
-                ld_dev2(p + z0, d, h[d].x, h[d].y);
-            } else if (cz(d) == 1) {
-                h[d] = ld_dev_pair(p + nb0.Z[0], p + z0, d);
-            } else {
-                h[d] = ld_dev_pair(p + z0 + 1, p + zp1, d);
-            }
-        }
-        bool fluid0 = true, fluid1 = true;
-        const bool face = on_walled_face(P, x, y, z0) || on_walled_face(P, x, y, z0 + 1);
-        if ((fl0 | fl1 | (int)face) != 0) {
-            fluid0 = resolve_state<M>(P, S, idx0, x, y, z0, fl0, nb0, Lane<0>{h});
-            Nbr nb1 = nb0;
-            nb1.Z[0] = z0;
-            nb1.Z[1] = z0 + 1;
-            nb1.Z[2] = zp1;
-            fluid1 = resolve_state<M>(P, S, idx0 + 1, x, y, z0 + 1, fl1, nb1, Lane<1>{h});
-        }
-        if constexpr (OUT != OUT_NONE) {
-            float f[Q];
-#pragma unroll
-            for (int d = 0; d < Q; ++d) f[d] = h[d].x;
-            emit<M, FM, OUT>(P, out, idx0, !fluid0, f, cons);
-#pragma unroll
-            for (int d = 0; d < Q; ++d) f[d] = h[d].y;
-            emit<M, FM, OUT>(P, out, idx0 + 1, !fluid1, f, cons);
-        }
-        M::template collide2<FM>(P, idx0, h, [&](int d, float2 v) {
-            st_dev2(S.dst[d] + idx0, d, fluid0 ? v.x : M::solid(P, d), fluid1 ? v.y : M::solid(P, d));
-        });
-    }
+    if (idx0 < P.n) step_pair<M, FM, OUT>(P, S, out, idx0, cons);
     if constexpr ((OUT & OUT_SUMS) != 0) block_sum5(cons, out.partials);
 }
 
-// Step from PRE: read f_n in place, collide, write P_n.  S.src holds the
-// buffer base pointers (direction d at S.src[d]).
+// Step from PRE for one cell: read f_n in place, collide, write P_n.
+template <class M, int FM, int OUT>
+__device__ __forceinline__ void collide_single(const Params& P, const Streams<typename M::T>& S,
+                                               const Outputs<typename M::C>& out, int idx, double* cons)
+{
+    using C = typename M::C;
+    const int type = P.has_flags ? (P.flags[idx] & 3) : CELL_FLUID;
+    C f[Q];
+#pragma unroll
+    for (int d = 0; d < Q; ++d) f[d] = M::load(S.src[d] + idx, d);
+    if (type == CELL_SOLID) {
+        emit<M, FM, OUT>(P, out, idx, true, f, cons);
+        store_solid<M>(P, S, idx);
+    } else {
+        emit<M, FM, OUT>(P, out, idx, false, f, cons);
+        M::template collide<FM>(P, idx, f);
+        store_all<M>(S, idx, f);
+    }
+}
+
+// Step from PRE: S.src holds the buffer base pointers (direction d at S.src[d]).
 template <class M, int FM, int OUT>
 __global__ void __launch_bounds__(256) k_collide_local(Params P, Streams<typename M::T> S,
                                                        Outputs<typename M::C> out)
 {
-    using C = typename M::C;
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     double cons[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    if (idx < P.n) {
-        const int type = P.has_flags ? (P.flags[idx] & 3) : CELL_FLUID;
-        C f[Q];
-#pragma unroll
-        for (int d = 0; d < Q; ++d) f[d] = M::load(S.src[d] + idx, d);
-        if (type == CELL_SOLID) {
-            emit<M, FM, OUT>(P, out, idx, true, f, cons);
-            store_solid<M>(P, S, idx);
-        } else {
-            emit<M, FM, OUT>(P, out, idx, false, f, cons);
-            M::template collide<FM>(P, idx, f);
-            store_all<M>(S, idx, f);
-        }
-    }
+    if (idx < P.n) collide_single<M, FM, OUT>(P, S, out, idx, cons);
     if constexpr ((OUT & OUT_SUMS) != 0) block_sum5(cons, out.partials);
 }
 

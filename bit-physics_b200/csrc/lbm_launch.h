@@ -46,6 +46,17 @@ cudaError_t launch_feq_init(int storage, const Params& P, const double* rho, con
 cudaError_t launch_mark_near_solid(const Params& P, uint8_t* flags, uint32_t* bbmask, cudaStream_t s);
 cudaError_t launch_reduce_partials(const double* partials, int nblocks, double* out5, cudaStream_t s);
 
+// Batched step (one launch for many lattices): records and items in device
+// memory, see lbm_batch.cuh.  `records` points to BatchLattice<T> for the
+// storage's element type.
+// sched: BatchSched (the pair schedules need f32/f16/bf16 storage and the
+// force-free or uniform force model); collide != 0 runs the in-place collide
+// of the first step, with items of `span` cells.
+cudaError_t launch_batch_step(int storage, int force_mode, int sched, bool collide, const void* records,
+                              const void* items, int nitems, int span, int phase, int grid, int block,
+                              cudaStream_t s);
+size_t batch_record_bytes(int storage);
+
 // TMA-staged step (lbm_tma.cu): tile plan for a lattice (stages == 0 when the
 // path does not apply) and the launch.
 TileCfg plan_tma(int storage, int nx, int ny, int nz, int* grid, int device);

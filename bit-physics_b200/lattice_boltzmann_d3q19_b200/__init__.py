@@ -17,6 +17,6 @@ from __future__ import annotations
 from . import _native
 from ._native import LbmError, device_count
 from .constants import C, CS2, OPP, VELOCITIES, WEIGHTS, W
-from .engine import Lattice
+from .engine import Batch, Lattice
 
-__all__ = ["C", "CS2", "Lattice", "LbmError", "OPP", "VELOCITIES", "W", "WEIGHTS", "_native", "device_count"]
+__all__ = ["Batch", "C", "CS2", "Lattice", "LbmError", "OPP", "VELOCITIES", "W", "WEIGHTS", "_native", "device_count"]

@@ -28,6 +28,7 @@ STORAGE = {"f64": 0, "f32": 1, "f16": 2, "bf16": 3}
 FORCE = {"none": 0, "uniform": 1, "field": 2, "drag": 3}
 FACES = {"x-": 0, "x+": 1, "y-": 2, "y+": 3, "z-": 4, "z+": 5}
 STAGING = {"auto": 0, "registers": 1, "tma": 2}
+SCHEDULES = {"single": 0, "pair_scalar": 1, "pair_mixed": 2}
 CELL_FLUID, CELL_SOLID, CELL_INFLOW, CELL_OUTFLOW = 0, 1, 2, 3
 
 
@@ -102,6 +103,16 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "lbm_stream_dev": ([_h, _h, _i, _i, _i, _h], C.c_int),
     "lbm_bgk_step_dev": ([_h, _h, C.c_double, _h, _i, _i, _i, _h], C.c_int),
     "lbm_bounce_back_y_walls_dev": ([_h, _h, _i, _i, _i, _dp, _dp, _h], C.c_int),
+    "lbm_batch_create": ([C.POINTER(LbmDesc), _i, C.POINTER(_h)], C.c_int),
+    "lbm_batch_destroy": ([_h], C.c_int),
+    "lbm_batch_count": ([_h], C.c_int),
+    "lbm_batch_lattice": ([_h, _i, C.POINTER(_h)], C.c_int),
+    "lbm_batch_set_schedule": ([_h, _i, _i, _i], C.c_int),
+    "lbm_batch_get_schedule": ([_h, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)], C.c_int),
+    "lbm_batch_step": ([_h, _i], C.c_int),
+    "lbm_batch_step_unbatched": ([_h, _i], C.c_int),
+    "lbm_batch_autotune": ([_h, _i, _dp], C.c_int),
+    "lbm_batch_synchronize": ([_h], C.c_int),
     "lbm_conservation_noalloc": ([_h, _h, _i, _i, _i, _h, _h], C.c_int),
     "lbm_last_error": ([], C.c_char_p),
     "lbm_version": ([], C.c_int),

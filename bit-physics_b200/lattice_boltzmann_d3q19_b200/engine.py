@@ -92,6 +92,7 @@ class Lattice:
             raise ValueError(f"staging must be one of {sorted(N.STAGING)}")
         d.staging = N.STAGING[staging]
         self.desc = d
+        self._owned = True
         h = C.c_void_p()
         N.check(N.lib().lbm_create(C.byref(d), C.byref(h)))
         self._h = h
@@ -109,9 +110,9 @@ class Lattice:
 
     # -- lifetime -----------------------------------------------------------
     def close(self) -> None:
-        if getattr(self, "_h", None) is not None and self._h.value:
+        if getattr(self, "_h", None) is not None and self._h.value and getattr(self, "_owned", True):
             N.lib().lbm_destroy(self._h)
-            self._h = C.c_void_p()
+        self._h = C.c_void_p()
 
     def __del__(self):
         try:
@@ -237,3 +238,109 @@ class Lattice:
 
     def synchronize(self) -> None:
         N.check(N.lib().lbm_synchronize(self._h))
+
+
+class Batch:
+    """Independent lattices advanced together, one kernel launch per step.
+
+    ``specs`` is a list of dicts of ``Lattice`` keyword arguments (``shape``
+    and ``tau`` required); all lattices share storage and force model.
+    ``batch[i]`` is a ``Lattice`` view of lattice i (state transfer,
+    readback, flags) owned by the batch."""
+
+    def __init__(self, specs):
+        specs = list(specs)
+        if not specs:
+            raise ValueError("a batch needs at least one lattice")
+        descs = (N.LbmDesc * len(specs))()
+        self._views_kw = []
+        for k, spec in enumerate(specs):
+            kw = dict(spec)
+            shape, tau = kw.pop("shape"), kw.pop("tau")
+            d = N.LbmDesc()
+            N.check(N.lib().lbm_desc_init(C.byref(d)))
+            nx, ny, nz = (int(v) for v in shape)
+            d.nx, d.ny, d.nz = nx, ny, nz
+            d.storage = N.STORAGE[kw.get("storage", "f64")]
+            d.periodic = _periodic_mask(kw.get("periodic", (True, True, True)))
+            d.force_mode = N.FORCE[kw.get("force_mode", "none")]
+            d.tau = float(tau)
+            wu = Lattice._wall_array(kw.get("wall_velocity"))
+            for j in range(18):
+                d.wall_velocity[j] = float(wu[j // 3, j % 3])
+            bf = kw.get("body_force", (0.0, 0.0, 0.0))
+            iu = kw.get("inflow_u", (0.0, 0.0, 0.0))
+            for j in range(3):
+                d.body_force[j] = float(bf[j])
+                d.inflow_u[j] = float(iu[j])
+            d.drag_k = float(kw.get("drag_k", 0.0))
+            d.inflow_rho = float(kw.get("inflow_rho", 1.0))
+            d.device = int(kw.get("device", 0))
+            descs[k] = d
+            self._views_kw.append(((nx, ny, nz), float(tau), kw))
+        h = C.c_void_p()
+        N.check(N.lib().lbm_batch_create(descs, len(specs), C.byref(h)))
+        self._h = h
+        self._views = []
+        for k, (shape, tau, kw) in enumerate(self._views_kw):
+            lh = C.c_void_p()
+            N.check(N.lib().lbm_batch_lattice(self._h, k, C.byref(lh)))
+            view = Lattice.__new__(Lattice)
+            view.shape = shape
+            view.n = shape[0] * shape[1] * shape[2]
+            view.storage = kw.get("storage", "f64")
+            view.force_mode = kw.get("force_mode", "none")
+            view.desc = descs[k]
+            view._owned = False
+            view._h = lh
+            self._views.append(view)
+
+    def __len__(self):
+        return len(self._views)
+
+    def __getitem__(self, i) -> Lattice:
+        return self._views[i]
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            for v in self._views:
+                v._h = C.c_void_p()
+            N.lib().lbm_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def step(self, n_steps: int = 1) -> None:
+        N.check(N.lib().lbm_batch_step(self._h, int(n_steps)))
+
+    def step_unbatched(self, n_steps: int = 1) -> None:
+        N.check(N.lib().lbm_batch_step_unbatched(self._h, int(n_steps)))
+
+    def set_schedule(self, schedule: str = "single", block: int = 256, grid: int = 0) -> None:
+        N.check(N.lib().lbm_batch_set_schedule(self._h, N.SCHEDULES[schedule], int(block), int(grid)))
+
+    def schedule(self) -> tuple[str, int, int]:
+        s, b, g = C.c_int32(), C.c_int32(), C.c_int32()
+        N.check(N.lib().lbm_batch_get_schedule(self._h, C.byref(s), C.byref(b), C.byref(g)))
+        name = {v: k for k, v in N.SCHEDULES.items()}[s.value]
+        return name, b.value, g.value
+
+    def autotune(self, trial_steps: int = 20) -> float:
+        """Time every schedule, keep the fastest; returns its ms per step.
+        The lattices' states are restored afterwards."""
+        ms = C.c_double()
+        N.check(N.lib().lbm_batch_autotune(self._h, int(trial_steps), C.byref(ms)))
+        return ms.value
+
+    def synchronize(self) -> None:
+        N.check(N.lib().lbm_batch_synchronize(self._h))

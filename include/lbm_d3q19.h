@@ -195,6 +195,37 @@ int lbm_bounce_back_y_walls_dev(const double* f, double* f_out, int32_t nx, int3
                                 int32_t nz, const double* wall_velocity_top,
                                 const double* wall_velocity_bottom, void* stream);
 
+/* ---- batches: many independent lattices, one launch per step -----------
+ * The batched ensemble the reference does not have: lattices of different
+ * sizes and parameters (same storage and force model) advanced together by
+ * one persistent kernel launch per step, replayed from a CUDA graph.  Each
+ * lattice is an ordinary handle (lbm_batch_lattice) for state transfer and
+ * readback; the batch owns them and their stream. */
+typedef struct lbm_batch lbm_batch;
+
+#define LBM_SCHED_SINGLE 0      /* one cell per thread                              */
+#define LBM_SCHED_PAIR_SCALAR 1 /* two cells per thread, f32x2 collision            */
+#define LBM_SCHED_PAIR_MIXED 2  /* as 1, vector memory access where nz is even      */
+
+int lbm_batch_create(const lbm_desc* descs, int32_t count, lbm_batch** out);
+int lbm_batch_destroy(lbm_batch* b);
+int lbm_batch_count(const lbm_batch* b);
+/* Borrowed handle of lattice i (valid until lbm_batch_destroy). */
+int lbm_batch_lattice(lbm_batch* b, int32_t i, lbm_lattice** out);
+/* Work schedule: sched LBM_SCHED_*, threads per block (multiple of 32, <= 256),
+ * grid = blocks of the persistent launch (0: 4 per SM). */
+int lbm_batch_set_schedule(lbm_batch* b, int32_t sched, int32_t block, int32_t grid);
+int lbm_batch_get_schedule(const lbm_batch* b, int32_t* sched, int32_t* block, int32_t* grid);
+/* Advance every lattice n_steps: one launch per step, steady-state steps
+ * replayed from a captured two-step CUDA graph. */
+int lbm_batch_step(lbm_batch* b, int32_t n_steps);
+/* The same with one launch per lattice and step (for comparison). */
+int lbm_batch_step_unbatched(lbm_batch* b, int32_t n_steps);
+/* Time every schedule on trial_steps steps, keep the fastest (ms per step in
+ * *best_ms); the lattices' states are saved before and restored after. */
+int lbm_batch_autotune(lbm_batch* b, int32_t trial_steps, double* best_ms);
+int lbm_batch_synchronize(lbm_batch* b);
+
 /* ---- without device allocation ----------------------------------------- */
 /* No counterpart in the reference.  FP64 sums {sum rho, sum m_x, sum m_y,
  * sum m_z} of a population array f (19, nx, ny, nz, f64, device memory) over
