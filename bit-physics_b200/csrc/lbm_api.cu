@@ -9,9 +9,11 @@
 #include <vector>
 
 #include "lbm_d3q19.h"
+#include "lbm_handle.h"
 #include "lbm_launch.h"
 
 using namespace lbm;
+using namespace lbm::api;
 
 namespace {
 thread_local std::string g_err;
@@ -23,7 +25,8 @@ int lbm::set_error(int code, const char* message)
     return code;
 }
 
-namespace {
+namespace lbm {
+namespace api {
 
 int fail(int code, const char* fmt, ...)
 {
@@ -45,11 +48,10 @@ int cuda_fail(cudaError_t e, const char* what)
     return fail(LBM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
-#define CK(call, what)                                   \
-    do {                                                 \
-        cudaError_t e_ = (call);                         \
-        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
-    } while (0)
+}  // namespace api
+}  // namespace lbm
+
+namespace {
 
 size_t storage_bytes(int storage)
 {
@@ -102,43 +104,12 @@ bool dims_ok(long long nx, long long ny, long long nz)
 
 }  // namespace
 
-struct lbm_lattice {
-    lbm_desc desc{};
-    int storage = 0;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    int n = 0;
-    size_t elem = 0;
-    void* buf[2] = {nullptr, nullptr};
-    int cur = 0;
-    bool pre = true;
-    uint8_t* flags = nullptr;
-    uint32_t* bbmask = nullptr; // (n) bounce-back masks, allocated with the flags
-    bool has_flags = false;
-    void* force = nullptr;   // (3, n) double (f64 storage) or float
-    float* poro = nullptr;   // (n)
-    void* rho = nullptr;     // readback buffers, double (f64 storage) or float
-    void* u = nullptr;
-    double* partials = nullptr;
-    double* sums = nullptr;  // 5 doubles
-    int partial_blocks = 0;
-    double* staging = nullptr; // (19, n) f64, allocated on first use
-    double* monitor = nullptr; // (monitor_cap, 5) per-step sums of lbm_step_monitor
-    int monitor_cap = 0;
-    int64_t steps = 0;
-    int block = 256;
-    int vec = 1; // cells per thread of the fused step kernel
-    int* err = nullptr; // device error word (pipeline wait timeouts)
-    bool use_tma = false;
-    int tma_grid = 0;
-    TileCfg tile{};
-    Params P{};
-};
 
 namespace {
 
 void rebuild_params(lbm_lattice* h)
 {
+    h->params_version += 1;  // any captured step graph is stale now
     Params& P = h->P;
     const lbm_desc& d = h->desc;
     init_geometry(P, d.nx, d.ny, d.nz);
@@ -175,8 +146,10 @@ void rebuild_params(lbm_lattice* h)
     P.pref = (float)(1.0 - 0.5 / d.tau);
 }
 
-cudaError_t launch(lbm_lattice* h, int kernel, const void* src, void* dst, bool post, double* f_out, void* rho,
-                   void* u, double* partials, int* grid_used = nullptr)
+}  // namespace
+
+cudaError_t lbm::api::launch(lbm_lattice* h, int kernel, const void* src, void* dst, bool post, double* f_out,
+                             void* rho, void* u, double* partials, int* grid_used)
 {
     LaunchArgs a;
     a.P = h->P;
@@ -201,6 +174,8 @@ cudaError_t launch(lbm_lattice* h, int kernel, const void* src, void* dst, bool 
     return launch_fast(h->storage, kernel, h->desc.force_mode, a);
 }
 
+namespace {
+
 int ensure_staging(lbm_lattice* h)
 {
     if (h->staging) return LBM_OK;
@@ -208,7 +183,9 @@ int ensure_staging(lbm_lattice* h)
     return LBM_OK;
 }
 
-int check_handle(const lbm_lattice* h)
+}  // namespace
+
+int lbm::api::check_handle(const lbm_lattice* h)
 {
     if (!h) return fail(LBM_ERR_INVALID, "null lattice handle");
     CK(cudaSetDevice(h->desc.device), "cudaSetDevice");
@@ -217,7 +194,7 @@ int check_handle(const lbm_lattice* h)
 
 // Advance one step; rho/u/partials receive the readback of the state
 // before the step (optional); *blocks (optional) the number of partials written.
-int advance(lbm_lattice* h, void* rho, void* u, double* partials, int* blocks = nullptr)
+int lbm::api::advance(lbm_lattice* h, void* rho, void* u, double* partials, int* blocks)
 {
     const void* src = h->buf[h->cur];
     void* dst = h->buf[h->cur ^ 1];
@@ -229,6 +206,8 @@ int advance(lbm_lattice* h, void* rho, void* u, double* partials, int* blocks = 
     h->steps += 1;
     return LBM_OK;
 }
+
+namespace {
 
 // Copy a device readback pair (C = double or float) into host f64 arrays.
 int readback_to_host(lbm_lattice* h, const void* drho, const void* du, double* rho, double* u)
@@ -251,14 +230,30 @@ int readback_to_host(lbm_lattice* h, const void* drho, const void* du, double* r
     return LBM_OK;
 }
 
-int observe_rho_u(lbm_lattice* h, void* drho, void* du)
+}  // namespace
+
+int lbm::api::check_device_ptr(const lbm_lattice* h, const void* p, const char* what)
+{
+    if (!p) return LBM_OK;
+    cudaPointerAttributes attr{};
+    cudaError_t e = cudaPointerGetAttributes(&attr, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(LBM_ERR_INVALID, "%s is not a CUDA pointer", what);
+    }
+    const bool dev = attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+    if (!dev || (attr.type == cudaMemoryTypeDevice && attr.device != h->desc.device))
+        return fail(LBM_ERR_INVALID, "%s must be device memory of GPU %d", what, h->desc.device);
+    return LBM_OK;
+}
+
+int lbm::api::observe_rho_u(lbm_lattice* h, void* drho, void* du)
 {
     cudaError_t e = launch(h, KERNEL_OBSERVE, h->buf[h->cur], nullptr, !h->pre, nullptr, drho, du, nullptr);
     if (e != cudaSuccess) return cuda_fail(e, "observe kernel launch");
     return LBM_OK;
 }
 
-}  // namespace
 
 extern "C" {
 
@@ -383,6 +378,7 @@ int lbm_destroy(lbm_lattice* h)
     if (!h) return LBM_OK;
     cudaSetDevice(h->desc.device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->graph) cudaGraphExecDestroy(h->graph);
     void* ptrs[] = {h->buf[0], h->buf[1], h->flags, h->bbmask, h->force, h->poro, h->rho,
                     h->u, h->partials, h->sums, h->staging, h->monitor, h->err};
     for (void* p : ptrs)
@@ -595,12 +591,41 @@ int lbm_set_body_force(lbm_lattice* h, const double* f3)
     return LBM_OK;
 }
 
-static int check_force_ready(lbm_lattice* h)
+}  // extern "C"
+
+int lbm::api::check_force_ready(lbm_lattice* h)
 {
     if (h->desc.force_mode == LBM_FORCE_FIELD && !h->force)
         return fail(LBM_ERR_STATE, "LBM_FORCE_FIELD lattice has no force field (lbm_set_force_field)");
     if (h->desc.force_mode == LBM_FORCE_DRAG && !h->poro)
         return fail(LBM_ERR_STATE, "LBM_FORCE_DRAG lattice has no porosity field (lbm_set_porosity)");
+    return LBM_OK;
+}
+
+extern "C" {
+
+// Capture the two steady-state steps from the current buffer into a graph.
+static int capture_step_graph(lbm_lattice* h)
+{
+    if (h->graph) {
+        cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "graph capture begin");
+    const int c = h->cur;
+    cudaError_t e0 = launch(h, KERNEL_STEP, h->buf[c], h->buf[c ^ 1], false, nullptr, nullptr, nullptr, nullptr);
+    cudaError_t e1 = launch(h, KERNEL_STEP, h->buf[c ^ 1], h->buf[c], false, nullptr, nullptr, nullptr, nullptr);
+    cudaError_t e2 = cudaStreamEndCapture(h->stream, &g);
+    if (e0 != cudaSuccess || e1 != cudaSuccess || e2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return cuda_fail(e0 != cudaSuccess ? e0 : (e1 != cudaSuccess ? e1 : e2), "step graph capture");
+    }
+    cudaError_t e = cudaGraphInstantiate(&h->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "step graph instantiate");
+    h->graph_cur = c;
+    h->graph_version = h->params_version;
     return LBM_OK;
 }
 
@@ -610,7 +635,24 @@ int lbm_step(lbm_lattice* h, int32_t n_steps)
     if (rc) return rc;
     if (n_steps < 0) return fail(LBM_ERR_INVALID, "negative step count");
     if ((rc = check_force_ready(h))) return rc;
-    for (int32_t s = 0; s < n_steps; ++s)
+    int32_t s = 0;
+    // Launch-bound small lattices gain from replaying steady-state steps
+    // (two per replay) from a captured CUDA graph.
+    if (n_steps >= 8) {
+        while (s < n_steps && (h->pre || (h->graph && h->graph_version == h->params_version && h->cur != h->graph_cur))) {
+            if ((rc = advance(h, nullptr, nullptr, nullptr))) return rc;
+            ++s;
+        }
+        if (n_steps - s >= 2) {
+            if (!h->graph || h->graph_version != h->params_version || h->cur != h->graph_cur)
+                if ((rc = capture_step_graph(h))) return rc;
+            for (; s + 1 < n_steps; s += 2) {
+                CK(cudaGraphLaunch(h->graph, h->stream), "step graph launch");
+                h->steps += 2;
+            }
+        }
+    }
+    for (; s < n_steps; ++s)
         if ((rc = advance(h, nullptr, nullptr, nullptr))) return rc;
     return LBM_OK;
 }
@@ -624,6 +666,48 @@ int lbm_get_rho_u(lbm_lattice* h, double* rho, double* u)
     if ((rc = check_force_ready(h))) return rc;
     if ((rc = observe_rho_u(h, h->rho, h->u))) return rc;
     return readback_to_host(h, h->rho, h->u, rho, u);
+}
+
+int lbm_get_rho_u_dev(lbm_lattice* h, double* rho, double* u)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if ((rc = check_force_ready(h))) return rc;
+    if (!rho && !u) return LBM_OK;
+    if ((rc = check_device_ptr(h, rho, "rho")) || (rc = check_device_ptr(h, u, "u"))) return rc;
+    const size_t n = (size_t)h->n;
+    if (h->storage == LBM_STORAGE_F64) {
+        // the readback kernel writes both fields; borrow the handle's buffer
+        // for the one not asked for
+        return observe_rho_u(h, rho ? rho : h->rho, u ? u : h->u);
+    }
+    if ((rc = observe_rho_u(h, h->rho, h->u))) return rc;
+    if (rho) CK(launch_widen((const float*)h->rho, rho, n, h->stream), "rho widen");
+    if (u) CK(launch_widen((const float*)h->u, u, 3 * n, h->stream), "u widen");
+    return LBM_OK;
+}
+
+int lbm_set_porosity_dev(lbm_lattice* h, const float* alpha)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!alpha) return fail(LBM_ERR_INVALID, "null porosity field");
+    if (h->desc.force_mode != LBM_FORCE_DRAG)
+        return fail(LBM_ERR_STATE, "lattice was not created with LBM_FORCE_DRAG");
+    if ((rc = check_device_ptr(h, alpha, "alpha"))) return rc;
+    const size_t n = (size_t)h->n;
+    // range check on the device; the 5-double sum scratch holds the flag
+    int* bad = (int*)h->sums;
+    int flag = 0;
+    CK(cudaMemsetAsync(bad, 0, sizeof(int), h->stream), "flag clear");
+    CK(launch_check_unit_interval(alpha, h->n, bad, h->stream), "porosity check");
+    CK(cudaMemcpyAsync(&flag, bad, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "flag read");
+    CK(cudaStreamSynchronize(h->stream), "porosity check sync");
+    if (flag) return fail(LBM_ERR_INVALID, "porosity outside [0, 1] (or NaN)");
+    if (!h->poro) CK(cudaMalloc((void**)&h->poro, sizeof(float) * n), "porosity allocation");
+    CK(cudaMemcpyAsync(h->poro, alpha, sizeof(float) * n, cudaMemcpyDeviceToDevice, h->stream), "porosity copy");
+    rebuild_params(h);
+    return LBM_OK;
 }
 
 int lbm_run_capture(lbm_lattice* h, int32_t n_steps, int32_t every, double* rho_frames, double* u_frames)

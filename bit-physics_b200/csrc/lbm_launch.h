@@ -62,6 +62,29 @@ size_t batch_record_bytes(int storage);
 TileCfg plan_tma(int storage, int nx, int ny, int nz, int* grid, int device);
 cudaError_t launch_tma_step(int storage, int force_mode, const LaunchArgs& a);
 
+// Adjoint (lbm_adjoint.cu): one level over n cells.  Lambda buffers are
+// (19, n) of adjoint_elem_bytes(storage) elements (double for f64 storage,
+// float otherwise); level: AdjointLevel of lbm_adjoint.cuh.
+struct AdjointArgs {
+    Params P;
+    const void* src;         // stored state of the level
+    const void* Lin;         // Lambda_{k+1}
+    void* Lout;              // Lambda_k
+    const double* grad_rho;  // INIT seeds (nullable)
+    const double* grad_u;
+    double* dalpha;          // accumulated dL/dalpha (nullable)
+    double* grad_f0;         // FINAL: dL/df_0 (nullable)
+    const int* special;      // the cells k_adjoint_special handles (launch_list_special)
+    int n_special;
+    cudaStream_t stream;
+};
+cudaError_t launch_adjoint_level(int storage, int force_mode, int level, const AdjointArgs& a);
+size_t adjoint_elem_bytes(int storage);
+// Compact the special cells of a lattice into list (capacity n), *count on the device.
+cudaError_t launch_list_special(const Params& P, int* list, int* count, cudaStream_t s);
+cudaError_t launch_widen(const float* in, double* out, size_t count, cudaStream_t s);
+cudaError_t launch_check_unit_interval(const float* a, int n, int* flag, cudaStream_t s);
+
 // Record the calling thread's error message (lbm_last_error) and return code.
 int set_error(int code, const char* message);
 

@@ -9,6 +9,9 @@ package's step and state API:
   running as sm_100a kernels behind the C ABI of ``include/lbm_d3q19.h``;
 * ``Lattice``    -- a stateful lattice resident in HBM, stepped by one fused
   pull-stream + bounce-back + collide kernel per step;
+* ``Tape``       -- checkpointed forward + hand-written adjoint kernels, and
+  ``autograd.run``, its torch.autograd.Function (gradients w.r.t. the
+  porosity field and the initial populations);
 * ``sim``        -- the canonical Poiseuille / Couette runners.
 """
 
@@ -17,6 +20,7 @@ from __future__ import annotations
 from . import _native
 from ._native import LbmError, device_count
 from .constants import C, CS2, OPP, VELOCITIES, WEIGHTS, W
-from .engine import Batch, Lattice
+from .engine import Batch, Lattice, Tape
 
-__all__ = ["Batch", "C", "CS2", "Lattice", "LbmError", "OPP", "VELOCITIES", "W", "WEIGHTS", "_native", "device_count"]
+__all__ = ["Batch", "C", "CS2", "Lattice", "LbmError", "OPP", "Tape", "VELOCITIES", "W", "WEIGHTS", "_native",
+           "device_count"]

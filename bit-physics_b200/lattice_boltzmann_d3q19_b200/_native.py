@@ -114,6 +114,12 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "lbm_batch_autotune": ([_h, _i, _dp], C.c_int),
     "lbm_batch_synchronize": ([_h], C.c_int),
     "lbm_conservation_noalloc": ([_h, _h, _i, _i, _i, _h, _h], C.c_int),
+    "lbm_get_rho_u_dev": ([_h, _h, _h], C.c_int),
+    "lbm_set_porosity_dev": ([_h, _h], C.c_int),
+    "lbm_tape_forward": ([_h, _i, _i, C.POINTER(_h)], C.c_int),
+    "lbm_tape_backward": ([_h, _h, _h, _h, _h], C.c_int),
+    "lbm_tape_bytes": ([_h], C.c_int64),
+    "lbm_tape_destroy": ([_h], C.c_int),
     "lbm_last_error": ([], C.c_char_p),
     "lbm_version": ([], C.c_int),
     "lbm_device_count": ([], C.c_int),

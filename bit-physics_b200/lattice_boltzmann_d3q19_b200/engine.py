@@ -239,6 +239,67 @@ class Lattice:
     def synchronize(self) -> None:
         N.check(N.lib().lbm_synchronize(self._h))
 
+    # -- device pointers and the adjoint tape ----------------------------------
+    def rho_u_device(self, rho_ptr: int | None, u_ptr: int | None) -> None:
+        """Write rho (n) and u (3, n) as f64 to device addresses (integers,
+        e.g. torch ``tensor.data_ptr()``), enqueued on the lattice's stream."""
+        N.check(N.lib().lbm_get_rho_u_dev(self._h, C.c_void_p(rho_ptr) if rho_ptr else None,
+                                          C.c_void_p(u_ptr) if u_ptr else None))
+
+    def set_porosity_device(self, alpha_ptr: int) -> None:
+        """set_porosity from n float32 values at a device address."""
+        N.check(N.lib().lbm_set_porosity_dev(self._h, C.c_void_p(alpha_ptr)))
+
+    def tape(self, n_steps: int, checkpoint_every: int = 50) -> Tape:
+        """Run n_steps from the current (just set) populations, keeping the
+        checkpoints a backward pass needs; see ``Tape``."""
+        t = C.c_void_p()
+        N.check(N.lib().lbm_tape_forward(self._h, int(n_steps), int(checkpoint_every), C.byref(t)))
+        return Tape(self, t, int(n_steps), int(checkpoint_every))
+
+
+class Tape:
+    """Checkpoints of a forward run (``Lattice.tape``) and the adjoint pass
+    back through it.  Pointers are device addresses (integers)."""
+
+    def __init__(self, lattice: Lattice, handle: C.c_void_p, n_steps: int, checkpoint_every: int):
+        self.lattice = lattice  # the tape borrows the lattice: keep it alive
+        self._t = handle
+        self.n_steps = n_steps
+        self.checkpoint_every = checkpoint_every
+
+    @property
+    def nbytes(self) -> int:
+        return int(N.lib().lbm_tape_bytes(self._t))
+
+    def backward(self, grad_rho_ptr: int | None, grad_u_ptr: int | None, grad_alpha_ptr: int | None,
+                 grad_f0_ptr: int | None = None) -> None:
+        """dL/dalpha (n) and dL/df_0 (19, n), f64, from dL/drho (n) and dL/du
+        (3, n) of the final readback; enqueued on the lattice's stream."""
+        if not self._t:
+            raise N.LbmError(N.LBM_ERR_STATE, "tape is closed")
+        if not self.lattice._h.value:
+            raise N.LbmError(N.LBM_ERR_STATE, "the tape's lattice is closed")
+        vp = [C.c_void_p(p) if p else None for p in (grad_rho_ptr, grad_u_ptr, grad_alpha_ptr, grad_f0_ptr)]
+        N.check(N.lib().lbm_tape_backward(self._t, *vp))
+
+    def close(self) -> None:
+        if self._t:
+            N.lib().lbm_tape_destroy(self._t)
+            self._t = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
 
 class Batch:
     """Independent lattices advanced together, one kernel launch per step.

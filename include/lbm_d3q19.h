@@ -226,6 +226,37 @@ int lbm_batch_step_unbatched(lbm_batch* b, int32_t n_steps);
 int lbm_batch_autotune(lbm_batch* b, int32_t trial_steps, double* best_ms);
 int lbm_batch_synchronize(lbm_batch* b);
 
+/* ---- device-pointer transfers (for callers whose fields live on the GPU) --
+ * rho (n) and u (3, n) of the current state as f64 into device memory,
+ * enqueued on the lattice's stream (either pointer may be NULL). */
+int lbm_get_rho_u_dev(lbm_lattice* h, double* rho, double* u);
+/* lbm_set_porosity from device memory (n floats in [0, 1], checked). */
+int lbm_set_porosity_dev(lbm_lattice* h, const float* alpha);
+
+/* ---- adjoint: gradients through taped steps -------------------------------
+ * The differentiable run the reference does not have (its Warp kernels are
+ * not taped).  lbm_tape_forward runs n_steps from the lattice's current PRE
+ * state (populations set by lbm_set_populations / lbm_set_equilibrium /
+ * lbm_set_flags and not stepped since), exactly as lbm_step would, and keeps
+ * a copy of the state every checkpoint_every steps plus the final one.
+ * lbm_tape_backward takes the gradient of a loss L(rho_N, u_N) of the final
+ * readback -- dL/drho (n) and dL/du (3, n), f64 device arrays, either may be
+ * NULL for zero -- and runs the discrete adjoint of every step back to the
+ * start, recomputing the states between checkpoints with the step kernels.
+ * Outputs (f64 device arrays, overwritten; either may be NULL):
+ *   grad_alpha (n)     dL/dalpha for the drag model (zero for other models)
+ *   grad_f0 (19, n)    dL/df_0 of the initial populations
+ * The tape borrows the lattice: the lattice must outlive it, and a backward
+ * after a change of the lattice's flags, fields or parameters returns
+ * LBM_ERR_STATE.  Work is enqueued on the lattice's stream. */
+typedef struct lbm_tape lbm_tape;
+int lbm_tape_forward(lbm_lattice* h, int32_t n_steps, int32_t checkpoint_every, lbm_tape** out);
+int lbm_tape_backward(lbm_tape* t, const double* grad_rho, const double* grad_u, double* grad_alpha,
+                      double* grad_f0);
+/* Device bytes the tape holds (checkpoints, segment states, adjoint fields). */
+int64_t lbm_tape_bytes(const lbm_tape* t);
+int lbm_tape_destroy(lbm_tape* t);
+
 /* ---- without device allocation ----------------------------------------- */
 /* No counterpart in the reference.  FP64 sums {sum rho, sum m_x, sum m_y,
  * sum m_z} of a population array f (19, nx, ny, nz, f64, device memory) over
