@@ -430,6 +430,288 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# Other workloads (one JSON line each; single GPU)
+# ---------------------------------------------------------------------------
+def _device_time(fn, torch, stream):
+    """Milliseconds of device time of fn() bracketed by events on stream."""
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record(stream)
+    fn()
+    end.record(stream)
+    torch.cuda.synchronize()
+    return start.elapsed_time(end)
+
+
+def run_cavity(args):
+    """64^3 lid-driven cavity, tau 0.6, lid (0.05, 0, 0) on y+, reference wall
+    rule on all six faces, rest initial state: f32, f16 and f64 storage."""
+    import torch
+
+    import oracle as O
+    from lattice_boltzmann_d3q19_b200 import Lattice, geometry
+
+    shape, tau, steps = (64, 64, 64), 0.6, args.steps
+    kw = geometry.lid_driven_cavity(0.05)
+    stream = torch.cuda.Stream()
+    out = {}
+    n = int(np.prod(shape))
+    for storage in ("f32", "f16", "f64"):
+        lat = Lattice(shape, tau, storage=storage, **kw)
+        lat.set_stream(stream.cuda_stream)
+        lat.set_equilibrium()
+        lat.step(args.warmup)
+        ms = _device_time(lambda: lat.step(steps), torch, stream)
+        healthy = lat.check_health()
+        lat.close()
+        out[storage] = {"glups": n * steps / (ms / 1e3) / 1e9, "ms_per_step": ms / steps, "healthy": healthy,
+                        "hbm_frac": n * BYTES_PER_CELL[storage] / (ms / steps / 1e3) / 1e9 / peak_hbm()[0]}
+    cpu = O.OracleLattice(shape, tau, periodic=0, wall_velocity=Lattice._wall_array(kw["wall_velocity"]))
+    cpu.set_populations(O.feq_field(np.ones(shape), np.zeros((3, *shape))))
+    cpu_steps = min(steps, int(os.environ.get("LBM_CAVITY_CPU_STEPS", "200")))
+    t = time.perf_counter()
+    cpu.step(cpu_steps)
+    dt = time.perf_counter() - t
+    print(json.dumps({
+        "metric": "D3Q19 GLUPS, 64^3 lid-driven cavity", "workload": "cavity", "unit": "GLUPS",
+        "value": out["f32"]["glups"], "steps": steps, "warmup": args.warmup, "variants": out,
+        "cpu_baseline": {"value": n * cpu_steps / dt / 1e9, "unit": "GLUPS", "cores": O.num_threads(),
+                         "kind": "port", "sample": f"{cpu_steps} steps of the 64^3 cavity, f64 CPU oracle"},
+        "config": {"shape": shape, "tau": tau, "lid": 0.05, "walls": "all six faces, reference wall rule"},
+    }), flush=True)
+
+
+def channel_flags(shape, scale):
+    """The headline sphere channel's geometry on another grid: radii scaled."""
+    from lattice_boltzmann_d3q19_b200 import geometry
+
+    flags, _ = geometry.sphere_channel(shape, n_spheres=N_SPHERES, radius=(RADIUS[0] * scale, RADIUS[1] * scale),
+                                       seed=SEED)
+    return flags
+
+
+def run_sweep(args):
+    """Precision sweep: the sphere channel on 512 x 256 x 256 (the headline
+    geometry scaled by 2, radii U[8, 20]) at tau 0.51, 0.56 and 0.8; f32, f16
+    and bf16 storage against the f64 build of the same kernels after the same
+    steps (default 5000), from the inflow equilibrium.  Reports each run's
+    GLUPS, its velocity error over fluid cells (L2-relative and max-relative)
+    and the FP64 mass change.  LBM_SWEEP_SHAPE overrides the size."""
+    import torch
+
+    from lattice_boltzmann_d3q19_b200 import Lattice
+
+    shape = tuple(int(v) for v in os.environ.get("LBM_SWEEP_SHAPE", "512,256,256").split(","))
+    flags = channel_flags(shape, shape[0] / SHAPE[0])
+    fluid = flags != 1
+    n = int(np.prod(shape))
+    steps = args.steps
+    stream = torch.cuda.Stream()
+    results = []
+    for tau in (0.51, 0.56, 0.8):
+        row = {"tau": tau}
+        u64 = None
+        for storage in ("f64", "f32", "f16", "bf16"):
+            lat = Lattice(shape, tau, storage=storage, inflow_u=(INFLOW_U, 0.0, 0.0))
+            lat.set_stream(stream.cuda_stream)
+            lat.set_flags(flags)
+            lat.set_equilibrium(1.0, (INFLOW_U, 0.0, 0.0))
+            m0 = lat.conservation()[0]
+            ms = _device_time(lambda: lat.step(steps), torch, stream)
+            m1 = lat.conservation()[0]
+            healthy = lat.check_health()
+            _, u = lat.rho_u()
+            lat.close()
+            entry = {"glups": n * steps / (ms / 1e3) / 1e9, "healthy": healthy,
+                     "mass_change_rel": (m1 - m0) / m0}
+            if storage == "f64":
+                u64 = u
+            else:
+                du = (u - u64)[:, fluid]
+                ref = u64[:, fluid]
+                entry["u_err_l2_rel"] = float(np.linalg.norm(du) / np.linalg.norm(ref))
+                entry["u_err_max_rel"] = float(np.abs(du).max() / np.abs(ref).max())
+            row[storage] = entry
+            del u
+        results.append(row)
+    f16_over_f32 = [r["f16"]["glups"] / r["f32"]["glups"] for r in results]
+    print(json.dumps({
+        "metric": "precision sweep: GLUPS and velocity error vs the f64 build", "workload": "sweep",
+        "unit": "GLUPS", "value": statistics.median(r["f16"]["glups"] for r in results), "steps": steps,
+        "shape": shape, "f16_over_f32_glups": f16_over_f32, "results": results,
+        "config": {"geometry": "sphere channel scaled x2 (40 spheres, r U[8,20], seed 42)",
+                   "inflow_u": INFLOW_U, "initial": "inflow equilibrium"},
+    }), flush=True)
+
+
+def run_ensemble(args):
+    """64 independent lid-driven cavities, sizes U[32,128] per axis, tau
+    U[0.52,0.9], lid U[0.02,0.08] (seed 42), f16 deviation storage: one
+    launch per lattice and step, one batched launch per step (default
+    schedule), and the autotuned schedule."""
+    import torch
+
+    from lattice_boltzmann_d3q19_b200 import Batch, geometry
+
+    ens = geometry.cavity_ensemble(64, seed=SEED)
+    specs = []
+    for shape, tau, lid in ens:
+        kw = geometry.lid_driven_cavity(lid)
+        specs.append(dict(shape=shape, tau=tau, storage="f16", **kw))
+    cells = sum(int(np.prod(s)) for s, _, _ in ens)
+    out = {}
+    with Batch(specs) as b:
+        for k in range(len(b)):
+            b[k].set_equilibrium()
+        b.step(args.warmup)
+        b.synchronize()
+
+        def timed(fn):
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            fn()
+            b.synchronize()
+            return time.perf_counter() - t
+
+        dt = timed(lambda: b.step_unbatched(args.steps))
+        out["per_lattice_launches"] = {"glups": cells * args.steps / dt / 1e9, "launches_per_step": len(b)}
+        b.set_schedule("single", 256, 0)
+        b.step(2)
+        dt = timed(lambda: b.step(args.steps))
+        out["batched_default"] = {"glups": cells * args.steps / dt / 1e9, "schedule": list(b.schedule()),
+                                  "launches_per_step": 1}
+        ms = b.autotune(20)
+        b.step(2)
+        dt = timed(lambda: b.step(args.steps))
+        out["batched_autotuned"] = {"glups": cells * args.steps / dt / 1e9, "schedule": list(b.schedule()),
+                                    "autotune_ms_per_step": ms, "launches_per_step": 1}
+        healthy = all(b[k].check_health() for k in range(len(b)))
+    print(json.dumps({"metric": "D3Q19 GLUPS, batched ensemble of 64 cavities", "workload": "ensemble",
+                      "unit": "GLUPS", "value": out["batched_autotuned"]["glups"], "steps": args.steps,
+                      "cells": cells, "healthy": healthy, "variants": out,
+                      "speedup_autotuned_over_per_lattice": out["batched_autotuned"]["glups"]
+                      / out["per_lattice_launches"]["glups"]}), flush=True)
+
+
+ADJ_STEPS, ADJ_EVERY = 2000, 50
+
+
+def adjoint_shape():
+    return tuple(int(v) for v in os.environ.get("LBM_ADJ_SHAPE", "128,128,128").split(","))
+
+
+def adjoint_lattice(storage: str, alpha):
+    """Channel on alpha's grid (128^3): inflow u_x = 0.04 at x = 0,
+    zero-gradient outflow at the last x plane, walled y (no-slip), periodic
+    z, tau 0.6, porosity drag F = -beta(alpha) m with k = 0.05."""
+    from lattice_boltzmann_d3q19_b200 import Lattice
+
+    shape = alpha.shape
+    flags = np.zeros(shape, np.uint8)
+    flags[0] = 2
+    flags[-1] = 3
+    lat = Lattice(shape, 0.6, storage=storage, periodic=(True, False, True), force_mode="drag", drag_k=0.05,
+                  inflow_u=(0.04, 0.0, 0.0))
+    lat.set_flags(flags)
+    lat.set_porosity(alpha)
+    return lat
+
+
+def run_adjoint(args):
+    """Adjoint workload: d(kinetic energy in the last quarter of x after 2000
+    steps) / d(alpha) on the 128^3 FP32 channel, alpha = Gaussian-filtered
+    (sigma 4, periodic) noise in [0, 1], checkpoints every 50 steps.  Times
+    the plain forward, the taped forward and the backward (segment recompute
+    + adjoint kernels); checks the gradient against central differences of
+    the f64 forward along 16 seeded random directions.  LBM_ADJ_SHAPE,
+    LBM_ADJ_STEPS and LBM_ADJ_DIRECTIONS override the size, the step count
+    and the number of directions (small cases for profiling)."""
+    import torch
+
+    from lattice_boltzmann_d3q19_b200 import geometry
+
+    shape = adjoint_shape()
+    box = (3 * shape[0] // 4, shape[0])
+    steps = int(os.environ.get("LBM_ADJ_STEPS", ADJ_STEPS))
+    n = int(np.prod(shape))
+    alpha = geometry.smooth_porosity(shape, sigma=4.0, seed=SEED)
+    stream = torch.cuda.Stream()  # torch work and the lattices share it
+
+    def box_energy(rho, u):
+        x0, x1 = box
+        return 0.5 * (rho[x0:x1] * (u[:, x0:x1] ** 2).sum(0)).sum()
+
+    def gradient(storage):
+        lat = adjoint_lattice(storage, alpha)
+        lat.set_stream(stream.cuda_stream)
+        lat.set_equilibrium()
+        lat.step(3)
+        lat.set_equilibrium()
+        t_fwd = _device_time(lambda: lat.step(steps), torch, stream)
+        lat.set_equilibrium()
+        holder = {}
+        t_tape = _device_time(lambda: holder.update(tape=lat.tape(steps, ADJ_EVERY)), torch, stream)
+        tape = holder["tape"]
+        rho = torch.empty(shape, dtype=torch.float64, device="cuda")
+        u = torch.empty((3, *shape), dtype=torch.float64, device="cuda")
+        lat.rho_u_device(rho.data_ptr(), u.data_ptr())
+        r = rho.clone().requires_grad_(True)
+        v = u.clone().requires_grad_(True)
+        L = box_energy(r, v)
+        L.backward()
+        ga = torch.empty(shape, dtype=torch.float64, device="cuda")
+        t_bwd = _device_time(lambda: tape.backward(r.grad.data_ptr(), v.grad.data_ptr(), ga.data_ptr()), torch,
+                             stream)
+        out = {"loss": float(L.detach()), "forward_ms": t_fwd, "taped_forward_ms": t_tape, "backward_ms": t_bwd,
+               "tape_gb": tape.nbytes / 1e9, "forward_glups": n * steps / (t_fwd / 1e3) / 1e9,
+               "adjoint_over_forward": t_bwd / t_fwd, "healthy": lat.check_health()}
+        tape.close()
+        lat.close()
+        return out, ga.cpu().numpy()
+
+    with torch.cuda.stream(stream):
+        res32, g32 = gradient("f32")
+        res64, g64 = gradient("f64")
+    # central differences of the f64 forward; the perturbed alpha is stored
+    # as float32, so each difference is taken against the stored step
+    lat = adjoint_lattice("f64", alpha)
+    rng = np.random.default_rng(SEED)
+    n_dir = int(os.environ.get("LBM_ADJ_DIRECTIONS", "16"))
+    errs32, errs64 = [], []
+
+    def loss_at(a):
+        lat.set_porosity(a)
+        lat.set_equilibrium()
+        lat.step(steps)
+        rho, u = lat.rho_u()
+        return float(box_energy(torch.from_numpy(rho), torch.from_numpy(u)))
+
+    for _ in range(n_dir):
+        d = 1e-3 * rng.standard_normal(shape)
+        ap = np.clip(alpha + d, 0, 1).astype(np.float32)
+        am = np.clip(alpha - d, 0, 1).astype(np.float32)
+        fd = loss_at(ap) - loss_at(am)
+        delta = ap.astype(np.float64) - am.astype(np.float64)
+        errs64.append(abs(float((g64 * delta).sum()) - fd) / abs(fd))
+        errs32.append(abs(float((g32 * delta).sum()) - fd) / abs(fd))
+    lat.close()
+    rel_l2 = float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64))
+    print(json.dumps({
+        "metric": "adjoint / forward time, FP32 porosity-drag channel", "workload": "adjoint",
+        "unit": "ratio", "value": res32["adjoint_over_forward"], "higher_is_better": False, "steps": steps,
+        "checkpoint_every": ADJ_EVERY, "f32": res32, "f64": res64,
+        "gradient_check": {"directions": n_dir, "per_cell_step": 1e-3, "fd_kind": "central, f64 forward",
+                           "max_rel_err_f32_adjoint": max(errs32, default=None),
+                           "max_rel_err_f64_adjoint": max(errs64, default=None),
+                           "f32_vs_f64_gradient_rel_l2": rel_l2},
+        "config": {"shape": shape, "tau": 0.6, "inflow_u": 0.04, "drag_k": 0.05, "walls": "y (no-slip)",
+                   "alpha": "gaussian-filtered noise, sigma 4, seed 42, [0, 1]",
+                   "loss": f"KE in x in [{box[0]}, {box[1]})"},
+    }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -442,6 +724,7 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cells-per-thread", type=int, default=0, choices=[0, 1, 2])
     ap.add_argument("--staging", default="auto", choices=["auto", "registers", "tma"])
+    ap.add_argument("--workload", default="channel", choices=["channel", "cavity", "sweep", "ensemble", "adjoint"])
     args = ap.parse_args()
     global CELLS_PER_THREAD, STAGING
     CELLS_PER_THREAD = args.cells_per_thread
@@ -453,6 +736,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.workload != "channel":
+        {"cavity": run_cavity, "sweep": run_sweep, "ensemble": run_ensemble,
+         "adjoint": run_adjoint}[args.workload](args)
         return
     run_ours(args, rank, world, local_rank)
 
