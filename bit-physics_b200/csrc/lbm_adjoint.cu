@@ -41,15 +41,16 @@ cudaError_t launch_level_m(int level, const AdjointArgs& a)
     const int block = 256;
     const int grid = grid_for(a.P.n, block);
     const int sb = 128, sg = grid_for(a.n_special, sb);
+    cudaStream_t ss = a.special_stream ? a.special_stream : a.stream;
     switch (level) {
     case ADJ_INIT:
         if (a.n_special > 0)
-            k_adjoint_special<M, FM, ADJ_INIT><<<sg, sb, 0, a.stream>>>(a.P, S, io, a.special, a.n_special);
+            k_adjoint_special<M, FM, ADJ_INIT><<<sg, sb, 0, ss>>>(a.P, S, io, a.special, a.n_special);
         k_adjoint_plain<M, FM, ADJ_INIT><<<grid, block, 0, a.stream>>>(a.P, S, io);
         break;
     case ADJ_STEP:
         if (a.n_special > 0)
-            k_adjoint_special<M, FM, ADJ_STEP><<<sg, sb, 0, a.stream>>>(a.P, S, io, a.special, a.n_special);
+            k_adjoint_special<M, FM, ADJ_STEP><<<sg, sb, 0, ss>>>(a.P, S, io, a.special, a.n_special);
         k_adjoint_plain<M, FM, ADJ_STEP><<<grid, block, 0, a.stream>>>(a.P, S, io);
         break;
     case ADJ_FINAL: k_adjoint_final<M, FM><<<grid, block, 0, a.stream>>>(a.P, S, io); break;

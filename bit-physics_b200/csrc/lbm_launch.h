@@ -77,6 +77,8 @@ struct AdjointArgs {
     const int* special;      // the cells k_adjoint_special handles (launch_list_special)
     int n_special;
     cudaStream_t stream;
+    cudaStream_t special_stream;  // where k_adjoint_special runs (NULL: stream); the
+                                  // caller orders the two (they touch disjoint cells)
 };
 cudaError_t launch_adjoint_level(int storage, int force_mode, int level, const AdjointArgs& a);
 size_t adjoint_elem_bytes(int storage);

@@ -29,6 +29,10 @@ struct lbm_tape {
     void* lam[2] = {nullptr, nullptr};
     int* special = nullptr;       // cells of k_adjoint_special (capacity n), then a count
     int n_special = 0;
+    // The special-cell kernel of a level runs on `side`, forked from and
+    // joined back into the lattice's stream, beside the plain-cell kernel.
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 namespace {
@@ -39,14 +43,28 @@ void free_tape(lbm_tape* t)
 {
     if (!t) return;
     cudaSetDevice(t->device);
+    if (t->side) cudaStreamSynchronize(t->side);
     if (t->arena) cudaFree(t->arena);
+    if (t->fork) cudaEventDestroy(t->fork);
+    if (t->join) cudaEventDestroy(t->join);
+    if (t->side) cudaStreamDestroy(t->side);
     delete t;
 }
 
 int level(lbm_tape* t, int kind, AdjointArgs& a)
 {
+    const bool fork = kind != ADJ_FINAL && a.n_special > 0;
+    if (fork) {
+        CK(cudaEventRecord(t->fork, a.stream), "fork record");
+        CK(cudaStreamWaitEvent(t->side, t->fork, 0), "fork wait");
+    }
+    a.special_stream = fork ? t->side : nullptr;
     cudaError_t e = launch_adjoint_level(t->h->storage, t->h->desc.force_mode, kind, a);
     if (e != cudaSuccess) return cuda_fail(e, "adjoint kernel launch");
+    if (fork) {
+        CK(cudaEventRecord(t->join, t->side), "join record");
+        CK(cudaStreamWaitEvent(a.stream, t->join, 0), "join wait");
+    }
     return LBM_OK;
 }
 
@@ -74,6 +92,13 @@ int lbm_tape_forward(lbm_lattice* h, int32_t n_steps, int32_t checkpoint_every, 
     t->n_steps = n_steps;
     t->every = every;
     t->state_bytes = h->elem * Q * (size_t)h->n;
+    cudaError_t es = cudaStreamCreateWithFlags(&t->side, cudaStreamNonBlocking);
+    if (es == cudaSuccess) es = cudaEventCreateWithFlags(&t->fork, cudaEventDisableTiming);
+    if (es == cudaSuccess) es = cudaEventCreateWithFlags(&t->join, cudaEventDisableTiming);
+    if (es != cudaSuccess) {
+        free_tape(t);
+        return cuda_fail(es, "tape stream / event creation");
+    }
     const size_t sb = round_up(t->state_bytes, 256);
     const size_t lb = round_up(adjoint_elem_bytes(h->storage) * Q * (size_t)h->n, 256);
     const size_t nstates = (size_t)nck + 1 + (size_t)(every - 1);
