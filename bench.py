@@ -168,6 +168,14 @@ CELLS_PER_THREAD = 0  # 0: the library's choice
 STAGING = "auto"
 
 
+def step_kernel(storage: str) -> str:
+    """Name of the step kernel a lattice of the headline shape runs."""
+    if STAGING == "tma":
+        return f"k_step_tma<{storage}>"
+    cpt = CELLS_PER_THREAD or (1 if storage == "f64" else 2)
+    return f"{'k_step2' if cpt == 2 else 'k_step'}<{storage}>"
+
+
 def make_lattice(storage: str, flags, device: int):
     from lattice_boltzmann_d3q19_b200 import Lattice
 
@@ -310,7 +318,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "frac": achieved / hbm,
         "traffic": None if tr is None else tr * n,
         "algorithmic_bytes_per_launch": n * bpc,
-        "kernel": f"k_step<{args.storage}> (fused pull-stream + boundary + BGK collide)",
+        "kernel": f"{step_kernel(args.storage)} (fused pull-stream + boundary + BGK collide)",
     }
 
     # variants and precision (every rank runs them; no collectives inside)
