@@ -170,7 +170,7 @@ STAGING = "auto"
 
 def step_kernel(storage: str) -> str:
     """Name of the step kernel a lattice of the headline shape runs."""
-    if STAGING == "tma":
+    if STAGING == "tma" and storage != "f64":
         return f"k_step_tma<{storage}>"
     cpt = CELLS_PER_THREAD or (1 if storage == "f64" else 2)
     return f"{'k_step2' if cpt == 2 else 'k_step'}<{storage}>"
@@ -179,8 +179,10 @@ def step_kernel(storage: str) -> str:
 def make_lattice(storage: str, flags, device: int):
     from lattice_boltzmann_d3q19_b200 import Lattice
 
+    # the TMA-staged kernel serves the f32-arithmetic storages only
+    staging = STAGING if storage != "f64" else "auto"
     lat = Lattice(SHAPE, TAU, storage=storage, inflow_u=(INFLOW_U, 0.0, 0.0), device=device,
-                  cells_per_thread=CELLS_PER_THREAD, staging=STAGING)
+                  cells_per_thread=CELLS_PER_THREAD, staging=staging)
     lat.set_flags(flags)
     lat.set_equilibrium(1.0, (INFLOW_U, 0.0, 0.0))
     return lat
