@@ -149,7 +149,7 @@ void rebuild_params(lbm_lattice* h)
 }  // namespace
 
 cudaError_t lbm::api::launch(lbm_lattice* h, int kernel, const void* src, void* dst, bool post, double* f_out,
-                             void* rho, void* u, double* partials, int* grid_used)
+                             void* rho, void* u, double* partials, int* grid_used, const PendingSums* prev)
 {
     LaunchArgs a;
     a.P = h->P;
@@ -160,6 +160,9 @@ cudaError_t lbm::api::launch(lbm_lattice* h, int kernel, const void* src, void* 
     a.rho = rho;
     a.u = u;
     a.partials = partials;
+    a.prev_partials = partials && prev ? prev->partials : nullptr;
+    a.prev_count = partials && prev ? prev->count : 0;
+    a.prev_sums = partials && prev ? prev->sums : nullptr;
     a.block = h->block;
     a.vec = kernel == KERNEL_STEP ? h->vec : 1;
     a.stream = h->stream;
@@ -194,12 +197,12 @@ int lbm::api::check_handle(const lbm_lattice* h)
 
 // Advance one step; rho/u/partials receive the readback of the state
 // before the step (optional); *blocks (optional) the number of partials written.
-int lbm::api::advance(lbm_lattice* h, void* rho, void* u, double* partials, int* blocks)
+int lbm::api::advance(lbm_lattice* h, void* rho, void* u, double* partials, int* blocks, const PendingSums* prev)
 {
     const void* src = h->buf[h->cur];
     void* dst = h->buf[h->cur ^ 1];
     cudaError_t e = launch(h, h->pre ? KERNEL_COLLIDE_LOCAL : KERNEL_STEP, src, dst, false, nullptr, rho, u, partials,
-                           blocks);
+                           blocks, prev);
     if (e != cudaSuccess) return cuda_fail(e, "step kernel launch");
     h->cur ^= 1;
     h->pre = false;
@@ -357,7 +360,7 @@ int lbm_create(const lbm_desc* desc, lbm_lattice** out)
                                                  "an even nz and nz * element size a multiple of 16 bytes"));
     h->partial_blocks = grid_for(h->n, h->block);
     if (h->partial_blocks < h->tma_grid) h->partial_blocks = h->tma_grid;
-    e = cudaMalloc((void**)&h->partials, sizeof(double) * 5 * (size_t)h->partial_blocks);
+    e = cudaMalloc((void**)&h->partials, sizeof(double) * 2 * 5 * (size_t)h->partial_blocks);
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->sums, sizeof(double) * 5);
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->err, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(h->err, 0, sizeof(int));
@@ -751,11 +754,16 @@ int lbm_step_monitor(lbm_lattice* h, int32_t n_steps, double* sums)
         CK(cudaMalloc((void**)&h->monitor, sizeof(double) * 5 * (size_t)n_steps), "monitor allocation");
         h->monitor_cap = n_steps;
     }
+    // Step s writes its per-block partials into one of two buffers; block 0 of
+    // step s + 1 reduces them into monitor row s; one reduction launch ends it.
+    PendingSums pend{nullptr, 0, nullptr};
     for (int32_t s = 0; s < n_steps; ++s) {
+        double* part = h->partials + (size_t)(s & 1) * 5 * h->partial_blocks;
         int blocks = 0;
-        if ((rc = advance(h, nullptr, nullptr, h->partials, &blocks))) return rc;
-        CK(launch_reduce_partials(h->partials, blocks, h->monitor + 5 * (size_t)s, h->stream), "partial reduction");
+        if ((rc = advance(h, nullptr, nullptr, part, &blocks, s > 0 ? &pend : nullptr))) return rc;
+        pend = PendingSums{part, blocks, h->monitor + 5 * (size_t)s};
     }
+    CK(launch_reduce_partials(pend.partials, pend.count, pend.sums, h->stream), "partial reduction");
     std::vector<double> tmp(5 * (size_t)n_steps);
     CK(cudaMemcpyAsync(tmp.data(), h->monitor, sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost, h->stream),
        "monitor copy");

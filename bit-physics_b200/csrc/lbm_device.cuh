@@ -468,9 +468,15 @@ struct ModeFast {
     // f32x2 arithmetic; force fields / porosity are read as (cell, cell + 1)
     // pairs, so cell0 must be even.  Opposite directions are paired through
     // p_d = h_d - h_opp(d) for the momentum sums.  sink(d, value) receives
-    // each direction's post-collision pair as soon as it is final.
+    // each direction's post-collision pair as soon as it is final; the
+    // pre-collision moments are returned (the FP64 monitor sums use them).
+    // Pre-collision moments of the two cells: density deviation and momentum.
+    struct Moments2 {
+        float2 rd, mx, my, mz;
+    };
+
     template <int FM, class Sink>
-    static __device__ __forceinline__ void collide2(const Params& P, int cell0, float2* h, Sink&& sink)
+    static __device__ __forceinline__ Moments2 collide2(const Params& P, int cell0, float2* h, Sink&& sink)
     {
         float2 rd = h[0];
 #pragma unroll
@@ -549,6 +555,7 @@ struct ModeFast {
             sink(d, h[d]);
             sink(d + 1, h[d + 1]);
         }
+        return {rd, mx, my, mz};
     }
 
     template <int FM>

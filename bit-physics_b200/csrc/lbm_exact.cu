@@ -21,7 +21,7 @@ static void launch_step_out(int kernel, const LaunchArgs& a, int grid)
 {
     using T = typename M::T;
     using C = typename M::C;
-    Outputs<C> out{(C*)a.rho, (C*)a.u, a.partials};
+    Outputs<C> out{(C*)a.rho, (C*)a.u, a.partials, a.prev_partials, a.prev_count, a.prev_sums};
     const Streams<T> S = make_streams<T>(a.src, a.dst, a.P.n);
     if (kernel == KERNEL_STEP)
         k_step<M, FM, OUT><<<grid, a.block, 0, a.stream>>>(a.P, S, out);
@@ -36,7 +36,7 @@ static cudaError_t launch_exact_fm(int kernel, const LaunchArgs& a)
     using M = ModeExact;
     const int grid = grid_for(a.P.n, a.block);
     if (kernel == KERNEL_OBSERVE) {
-        Outputs<double> out{(double*)a.rho, (double*)a.u, a.partials};
+        Outputs<double> out{(double*)a.rho, (double*)a.u, a.partials, a.prev_partials, a.prev_count, a.prev_sums};
         k_observe<M, FM><<<grid, a.block, 0, a.stream>>>(a.P, make_streams<double>(a.src, nullptr, a.P.n), a.post,
                                                           a.f_out, out);
         return cudaGetLastError();

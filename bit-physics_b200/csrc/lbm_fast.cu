@@ -10,7 +10,7 @@ template <class M, int FM, int OUT>
 static void launch_step_out(int kernel, const LaunchArgs& a, int grid)
 {
     using T = typename M::T;
-    Outputs<float> out{(float*)a.rho, (float*)a.u, a.partials};
+    Outputs<float> out{(float*)a.rho, (float*)a.u, a.partials, a.prev_partials, a.prev_count, a.prev_sums};
     const Streams<T> S = make_streams<T>(a.src, a.dst, a.P.n);
     if (kernel == KERNEL_STEP && a.vec == 2) {
         const int grid2 = grid_for(a.P.n / 2, a.block);
@@ -31,7 +31,7 @@ static cudaError_t launch_fast_t(int kernel, const LaunchArgs& a)
     using M = ModeFast<T>;
     const int grid = grid_for(a.P.n, a.block);
     if (kernel == KERNEL_OBSERVE) {
-        Outputs<float> out{(float*)a.rho, (float*)a.u, a.partials};
+        Outputs<float> out{(float*)a.rho, (float*)a.u, a.partials, a.prev_partials, a.prev_count, a.prev_sums};
         k_observe<M, FM><<<grid, a.block, 0, a.stream>>>(a.P, make_streams<T>(a.src, nullptr, a.P.n), a.post,
                                                           a.f_out, out);
         return cudaGetLastError();

@@ -26,9 +26,9 @@ struct lbm_lattice {
     float* poro = nullptr;   // (n)
     void* rho = nullptr;     // readback buffers, double (f64 storage) or float
     void* u = nullptr;
-    double* partials = nullptr;
+    double* partials = nullptr;  // 2 x partial_blocks rows of 5 (alternating in step_monitor)
     double* sums = nullptr;  // 5 doubles
-    int partial_blocks = 0;
+    int partial_blocks = 0;  // rows of partials of one launch (one per block, any kernel)
     double* staging = nullptr; // (19, n) f64, allocated on first use
     double* monitor = nullptr; // (monitor_cap, 5) per-step sums of lbm_step_monitor
     int monitor_cap = 0;
@@ -60,11 +60,20 @@ int check_handle(const lbm_lattice* h);
 // LBM_ERR_STATE when the force model's field has not been set.
 int check_force_ready(lbm_lattice* h);
 // One kernel of the handle's configuration (KernelKind) from src to dst.
+// Partials of an earlier launch that the next launch with partials reduces
+// (its block 0) into sums.
+struct PendingSums {
+    const double* partials;
+    int count;
+    double* sums;
+};
 cudaError_t launch(lbm_lattice* h, int kernel, const void* src, void* dst, bool post, double* f_out, void* rho,
-                   void* u, double* partials, int* grid_used = nullptr);
+                   void* u, double* partials, int* grid_used = nullptr, const PendingSums* prev = nullptr);
 // Advance the handle by one step (rho/u/partials: optional readback of the
-// state before the step; *blocks: the number of partials written).
-int advance(lbm_lattice* h, void* rho, void* u, double* partials, int* blocks = nullptr);
+// state before the step; *blocks: the number of partials written; prev:
+// with partials, earlier partials this step's kernel reduces as well).
+int advance(lbm_lattice* h, void* rho, void* u, double* partials, int* blocks = nullptr,
+            const PendingSums* prev = nullptr);
 // Readback of the current state into the handle's rho/u buffers.
 int observe_rho_u(lbm_lattice* h, void* drho, void* du);
 // LBM_OK when p is NULL or device (or managed) memory of the handle's GPU,

@@ -35,9 +35,12 @@ enum OutBits : int { OUT_NONE = 0, OUT_RHO_U = 1, OUT_SUMS = 2 };
 // FP64 conservation partials (mass or mass deviation, m_x, m_y, m_z, cells).
 template <class C>
 struct Outputs {
-    C* rho;           // (n)
-    C* u;             // (3, n)
-    double* partials; // (gridDim.x, 5)
+    C* rho;                                // (n)
+    C* u;                                  // (3, n)
+    double* partials;                      // (gridDim.x, 5)
+    const double* prev_partials = nullptr; // optional: partials of the previous launch on the
+    int prev_count = 0;                    // stream (prev_count rows), which block 0 reduces
+    double* prev_sums = nullptr;           // into prev_sums (5)
 };
 
 // Block-level FP64 reduction of 5 values, fixed tree (deterministic for a
@@ -64,8 +67,25 @@ __device__ __forceinline__ void block_sum5(double v[5], double* out)
             for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
         if (lane == 0)
 #pragma unroll
-            for (int k = 0; k < 5; ++k) out[blockIdx.x * 5 + k] = v[k];
+            for (int k = 0; k < 5; ++k) out[k] = v[k];
     }
+}
+
+// Grid total of the previous launch's partials, by block 0 of this launch
+// (launched after that one on the same stream, so the partials are complete
+// and visible): a fixed-order sum, deterministic, that overlaps the other
+// blocks' work instead of costing a launch of its own.  Call with every
+// thread of the block.
+template <class C>
+__device__ __forceinline__ void reduce_prev(const Outputs<C>& out)
+{
+    if (blockIdx.x != 0 || !out.prev_sums) return;
+    double w[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int b = threadIdx.x; b < out.prev_count; b += blockDim.x)
+#pragma unroll
+        for (int k = 0; k < 5; ++k) w[k] += out.prev_partials[(size_t)b * 5 + k];
+    block_sum5(w, out.prev_sums);
+    __syncthreads();  // the shared reduction array is reused by the caller
 }
 
 template <class M, int FM, int OUT>
@@ -132,10 +152,11 @@ __device__ __forceinline__ void step_single(const Params& P, const Streams<typen
 template <class M, int FM, int OUT>
 __global__ void __launch_bounds__(256) k_step(Params P, Streams<typename M::T> S, Outputs<typename M::C> out)
 {
+    if constexpr ((OUT & OUT_SUMS) != 0) reduce_prev(out);
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     double cons[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     if (idx < P.n) step_single<M, FM, OUT>(P, S, out, idx, cons);
-    if constexpr ((OUT & OUT_SUMS) != 0) block_sum5(cons, out.partials);
+    if constexpr ((OUT & OUT_SUMS) != 0) block_sum5(cons, out.partials + (size_t)blockIdx.x * 5);
 }
 
 // Fused step from POST, two z-adjacent cells (z0 even, z0 + 1) per thread, for
@@ -183,18 +204,29 @@ __device__ __forceinline__ void step_pair(const Params& P, const Streams<typenam
         nb1.Z[2] = zp1;
         fluid1 = resolve_state<M>(P, S, idx0 + 1, x, y, z0 + 1, fl1, nb1, Lane<1>{h});
     }
-    if constexpr (OUT != OUT_NONE) {
+    if constexpr ((OUT & OUT_RHO_U) != 0) {
         float f[Q];
 #pragma unroll
         for (int d = 0; d < Q; ++d) f[d] = h[d].x;
-        emit<M, FM, OUT>(P, out, idx0, !fluid0, f, cons);
+        emit<M, FM, OUT_RHO_U>(P, out, idx0, !fluid0, f, cons);
 #pragma unroll
         for (int d = 0; d < Q; ++d) f[d] = h[d].y;
-        emit<M, FM, OUT>(P, out, idx0 + 1, !fluid1, f, cons);
+        emit<M, FM, OUT_RHO_U>(P, out, idx0 + 1, !fluid1, f, cons);
     }
-    M::template collide2<FM>(P, idx0, h, [&](int d, float2 v) {
+    const auto mo = M::template collide2<FM>(P, idx0, h, [&](int d, float2 v) {
         st_dev2(S.dst[d] + idx0, d, fluid0 ? v.x : M::solid(P, d), fluid1 ? v.y : M::solid(P, d));
     });
+    if constexpr ((OUT & OUT_SUMS) != 0) {
+        // the collision's own pre-collision moments (density deviation,
+        // momentum), assigned: the caller's sums hold this pair only, so they
+        // are not live during the step
+        const double k0 = fluid0 ? 1.0 : 0.0, k1 = fluid1 ? 1.0 : 0.0;
+        cons[0] = k0 * (double)mo.rd.x + k1 * (double)mo.rd.y;
+        cons[1] = k0 * (double)mo.mx.x + k1 * (double)mo.mx.y;
+        cons[2] = k0 * (double)mo.my.x + k1 * (double)mo.my.y;
+        cons[3] = k0 * (double)mo.mz.x + k1 * (double)mo.mz.y;
+        cons[4] = k0 + k1;
+    }
 }
 
 // Two consecutive cells idx0, idx0 + 1 of any lattice (they may sit in
@@ -234,10 +266,11 @@ template <class M, int FM, int OUT>
 __global__ void __launch_bounds__(256, LBM_STEP2_MIN_BLOCKS) k_step2(Params P, Streams<typename M::T> S,
                                                                     Outputs<typename M::C> out)
 {
+    if constexpr ((OUT & OUT_SUMS) != 0) reduce_prev(out);
     const int idx0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
     double cons[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     if (idx0 < P.n) step_pair<M, FM, OUT>(P, S, out, idx0, cons);
-    if constexpr ((OUT & OUT_SUMS) != 0) block_sum5(cons, out.partials);
+    if constexpr ((OUT & OUT_SUMS) != 0) block_sum5(cons, out.partials + (size_t)blockIdx.x * 5);
 }
 
 // Step from PRE for one cell: read f_n in place, collide, write P_n.
@@ -265,10 +298,11 @@ template <class M, int FM, int OUT>
 __global__ void __launch_bounds__(256) k_collide_local(Params P, Streams<typename M::T> S,
                                                        Outputs<typename M::C> out)
 {
+    if constexpr ((OUT & OUT_SUMS) != 0) reduce_prev(out);
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     double cons[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     if (idx < P.n) collide_single<M, FM, OUT>(P, S, out, idx, cons);
-    if constexpr ((OUT & OUT_SUMS) != 0) block_sum5(cons, out.partials);
+    if constexpr ((OUT & OUT_SUMS) != 0) block_sum5(cons, out.partials + (size_t)blockIdx.x * 5);
 }
 
 // Current state without advancing it: f_n as f64 (optional; used for POST
@@ -308,7 +342,7 @@ __global__ void __launch_bounds__(256) k_observe(Params P, Streams<typename M::T
         if (out.rho) emit<M, FM, OUT_RHO_U>(P, out, idx, solid, f, cons);
         if (out.partials) emit<M, FM, OUT_SUMS>(P, out, idx, solid, f, cons);
     }
-    if (out.partials) block_sum5(cons, out.partials);
+    if (out.partials) block_sum5(cons, out.partials + (size_t)blockIdx.x * 5);
 }
 
 // Sum per-block partials in a fixed order (one block).

@@ -22,10 +22,13 @@ struct LaunchArgs {
     void* rho;          // optional readback (double for f64 storage, float otherwise)
     void* u;
     double* partials;   // optional per-block conservation partials (grid x 5)
+    const double* prev_partials;  // with partials: block 0 also reduces these prev_count rows
+    int prev_count;               // (the previous launch's partials) into prev_sums
+    double* prev_sums;
     int block;
     int vec;            // cells per thread of KERNEL_STEP (1, or 2 for ModeFast with nz even)
     cudaStream_t stream;
-    int* grid_used;     // optional: receives the launched grid size
+    int* grid_used;     // optional: receives the launched grid size (partial rows written)
     int tma_grid;       // > 0: KERNEL_STEP runs the TMA-staged kernel with this grid
     TileCfg tile;
 };

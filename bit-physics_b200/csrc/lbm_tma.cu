@@ -25,7 +25,7 @@ static cudaError_t tma_out(const LaunchArgs& a)
     const size_t smem = (size_t)a.tile.stages * a.tile.stage_elems * sizeof(T) + 128;
     cudaError_t e = allow_smem<T, FM, OUT>(smem);
     if (e != cudaSuccess) return e;
-    Outputs<float> out{(float*)a.rho, (float*)a.u, a.partials};
+    Outputs<float> out{(float*)a.rho, (float*)a.u, a.partials, a.prev_partials, a.prev_count, a.prev_sums};
     kern<<<a.tma_grid, TMA_THREADS, smem, a.stream>>>(a.P, make_streams<T>(a.src, a.dst, a.P.n), a.tile, out);
     if (a.grid_used) *a.grid_used = a.tma_grid;
     return cudaGetLastError();

@@ -124,6 +124,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(Params P, Streams<t
     // Ring base rounded up to 128 bytes (the launch allocates the slack): every
     // bulk-copy destination is then a multiple of the 16-byte row size.
     T* ring = reinterpret_cast<T*>((reinterpret_cast<uintptr_t>(tma_smem) + 127) & ~(uintptr_t)127);
+    if constexpr ((OUT & OUT_SUMS) != 0) reduce_prev(out);
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
@@ -212,7 +213,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(Params P, Streams<t
             if (lane == 0) mbar_arrive(&empty[s]);
         }
     }
-    if constexpr ((OUT & OUT_SUMS) != 0) block_sum5(cons, out.partials);
+    if constexpr ((OUT & OUT_SUMS) != 0) block_sum5(cons, out.partials + (size_t)blockIdx.x * 5);
 }
 
 }  // namespace lbm
