@@ -400,6 +400,15 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         rate, cores, steps, dt, sample = cpu_reference_rate(flags, float(os.environ.get("LBM_CPU_BUDGET_S", "15")),
                                                             args.steps)
         cpu = {"value": rate, "unit": "GLUPS", "cores": cores, "kind": "port", "sample": sample}
+        # the same restatement on one thread (the reference's CPU path is serial)
+        import oracle as O
+
+        O.set_num_threads(1)
+        try:
+            r1, _, s1, _, _ = cpu_reference_rate(flags, float(os.environ.get("LBM_CPU1_BUDGET_S", "8")), args.steps)
+        finally:
+            O.set_num_threads(cores)
+        cpu["single_thread"] = {"value": r1, "unit": "GLUPS", "cores": 1, "steps": s1}
 
     if dist_on:
         torch.distributed.barrier()
@@ -465,19 +474,27 @@ def run_cavity(args):
 
     shape, tau, steps = (64, 64, 64), 0.6, args.steps
     kw = geometry.lid_driven_cavity(0.05)
+    # the reference-exact proxy: x, z periodic, walls only in y (the
+    # reference's own wall rule), lid on y+
+    proxy = {"periodic": (True, False, True), "wall_velocity": {"y+": (0.05, 0.0, 0.0)}}
     stream = torch.cuda.Stream()
-    out = {}
+    out, out_proxy = {}, {}
     n = int(np.prod(shape))
-    for storage in ("f32", "f16", "f64"):
-        lat = Lattice(shape, tau, storage=storage, **kw)
+
+    def timed(storage, kwargs):
+        lat = Lattice(shape, tau, storage=storage, **kwargs)
         lat.set_stream(stream.cuda_stream)
         lat.set_equilibrium()
         lat.step(args.warmup)
         ms = _device_time(lambda: lat.step(steps), torch, stream)
         healthy = lat.check_health()
         lat.close()
-        out[storage] = {"glups": n * steps / (ms / 1e3) / 1e9, "ms_per_step": ms / steps, "healthy": healthy,
-                        "hbm_frac": n * BYTES_PER_CELL[storage] / (ms / steps / 1e3) / 1e9 / peak_hbm()[0]}
+        return {"glups": n * steps / (ms / 1e3) / 1e9, "ms_per_step": ms / steps, "healthy": healthy,
+                "hbm_frac": n * BYTES_PER_CELL[storage] / (ms / steps / 1e3) / 1e9 / peak_hbm()[0]}
+
+    for storage in ("f32", "f16", "f64"):
+        out[storage] = timed(storage, kw)
+        out_proxy[storage] = timed(storage, proxy)
     cpu = O.OracleLattice(shape, tau, periodic=0, wall_velocity=Lattice._wall_array(kw["wall_velocity"]))
     cpu.set_populations(O.feq_field(np.ones(shape), np.zeros((3, *shape))))
     cpu_steps = min(steps, int(os.environ.get("LBM_CAVITY_CPU_STEPS", "200")))
@@ -487,6 +504,7 @@ def run_cavity(args):
     print(json.dumps({
         "metric": "D3Q19 GLUPS, 64^3 lid-driven cavity", "workload": "cavity", "unit": "GLUPS",
         "value": out["f32"]["glups"], "steps": steps, "warmup": args.warmup, "variants": out,
+        "reference_exact_proxy": out_proxy,
         "cpu_baseline": {"value": n * cpu_steps / dt / 1e9, "unit": "GLUPS", "cores": O.num_threads(),
                          "kind": "port", "sample": f"{cpu_steps} steps of the 64^3 cavity, f64 CPU oracle"},
         "config": {"shape": shape, "tau": tau, "lid": 0.05, "walls": "all six faces, reference wall rule"},
@@ -522,7 +540,7 @@ def run_sweep(args):
     results = []
     for tau in (0.51, 0.56, 0.8):
         row = {"tau": tau}
-        u64 = None
+        rho64 = u64 = None
         for storage in ("f64", "f32", "f16", "bf16"):
             lat = Lattice(shape, tau, storage=storage, inflow_u=(INFLOW_U, 0.0, 0.0))
             lat.set_stream(stream.cuda_stream)
@@ -532,19 +550,22 @@ def run_sweep(args):
             ms = _device_time(lambda: lat.step(steps), torch, stream)
             m1 = lat.conservation()[0]
             healthy = lat.check_health()
-            _, u = lat.rho_u()
+            rho, u = lat.rho_u()
             lat.close()
             entry = {"glups": n * steps / (ms / 1e3) / 1e9, "healthy": healthy,
                      "mass_change_rel": (m1 - m0) / m0}
             if storage == "f64":
-                u64 = u
+                rho64, u64 = rho, u
             else:
                 du = (u - u64)[:, fluid]
                 ref = u64[:, fluid]
                 entry["u_err_l2_rel"] = float(np.linalg.norm(du) / np.linalg.norm(ref))
                 entry["u_err_max_rel"] = float(np.abs(du).max() / np.abs(ref).max())
+                dr = (rho - rho64)[fluid]
+                entry["rho_err_l2_rel"] = float(np.linalg.norm(dr) / np.linalg.norm(rho64[fluid]))
+                entry["rho_err_max_abs"] = float(np.abs(dr).max())
             row[storage] = entry
-            del u
+            del rho, u
         results.append(row)
     f16_over_f32 = [r["f16"]["glups"] / r["f32"]["glups"] for r in results]
     print(json.dumps({
