@@ -163,6 +163,8 @@ cudaError_t lbm::api::launch(lbm_lattice* h, int kernel, const void* src, void* 
     a.prev_partials = partials && prev ? prev->partials : nullptr;
     a.prev_count = partials && prev ? prev->count : 0;
     a.prev_sums = partials && prev ? prev->sums : nullptr;
+    a.first = 0;
+    a.count = -1;
     a.block = h->block;
     a.vec = kernel == KERNEL_STEP ? h->vec : 1;
     a.stream = h->stream;
@@ -796,6 +798,69 @@ int lbm_conservation(lbm_lattice* h, double* out4)
     out4[2] = s[2];
     out4[3] = s[3];
     return LBM_OK;
+}
+
+int lbm_conservation_planes(lbm_lattice* h, int32_t x0, int32_t x1, double* out4)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!out4) return fail(LBM_ERR_INVALID, "null output");
+    if (x0 < 0 || x1 > h->desc.nx || x0 >= x1) return fail(LBM_ERR_INVALID, "plane range [%d, %d) invalid", x0, x1);
+    if ((rc = check_force_ready(h))) return rc;
+    const int nynz = h->desc.ny * h->desc.nz;
+    LaunchArgs a{};
+    a.P = h->P;
+    a.src = h->buf[h->cur];
+    a.post = !h->pre;
+    a.partials = h->partials;
+    a.block = h->block;
+    a.vec = 1;
+    a.stream = h->stream;
+    a.first = x0 * nynz;
+    a.count = (x1 - x0) * nynz;
+    const cudaError_t e = h->storage == LBM_STORAGE_F64 ? launch_exact(KERNEL_OBSERVE, h->desc.force_mode, a)
+                                                        : launch_fast(h->storage, KERNEL_OBSERVE, h->desc.force_mode, a);
+    if (e != cudaSuccess) return cuda_fail(e, "conservation kernel");
+    CK(launch_reduce_partials(h->partials, grid_for(a.count, h->block), h->sums, h->stream), "partial reduction");
+    double s5[5];
+    CK(cudaMemcpyAsync(s5, h->sums, sizeof(s5), cudaMemcpyDeviceToHost, h->stream), "sum copy");
+    CK(cudaStreamSynchronize(h->stream), "sum sync");
+    out4[0] = h->storage == LBM_STORAGE_F64 ? s5[0] : s5[0] + s5[4];
+    out4[1] = s5[1];
+    out4[2] = s5[2];
+    out4[3] = s5[3];
+    return LBM_OK;
+}
+
+// Plane x of the stored array, directions in dir_mask, to or from a device
+// buffer (direction-major in increasing d, ny * nz elements each).
+static int plane_copy(lbm_lattice* h, int32_t x, uint32_t dir_mask, void* dev, bool get)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!dev) return fail(LBM_ERR_INVALID, "null plane buffer");
+    if (x < 0 || x >= h->desc.nx) return fail(LBM_ERR_INVALID, "plane %d outside [0, %d)", x, h->desc.nx);
+    if (dir_mask == 0 || dir_mask >= (1u << Q)) return fail(LBM_ERR_INVALID, "direction mask 0x%x invalid", dir_mask);
+    if ((rc = check_device_ptr(h, dev, "plane buffer"))) return rc;
+    const size_t plane = (size_t)h->desc.ny * h->desc.nz * h->elem;
+    char* base = (char*)h->buf[h->cur];
+    char* buf = (char*)dev;
+    size_t k = 0;
+    for (int d = 0; d < Q; ++d) {
+        if (!((dir_mask >> d) & 1u)) continue;
+        char* st = base + ((size_t)d * h->n + (size_t)x * h->desc.ny * h->desc.nz) * h->elem;
+        if (get) CK(cudaMemcpyAsync(buf + k * plane, st, plane, cudaMemcpyDeviceToDevice, h->stream), "plane copy");
+        else CK(cudaMemcpyAsync(st, buf + k * plane, plane, cudaMemcpyDeviceToDevice, h->stream), "plane copy");
+        ++k;
+    }
+    return LBM_OK;
+}
+
+int lbm_plane_get(lbm_lattice* h, int32_t x, uint32_t dir_mask, void* dst) { return plane_copy(h, x, dir_mask, dst, true); }
+
+int lbm_plane_put(lbm_lattice* h, int32_t x, uint32_t dir_mask, const void* src)
+{
+    return plane_copy(h, x, dir_mask, const_cast<void*>(src), false);
 }
 
 int lbm_check_health(lbm_lattice* h)

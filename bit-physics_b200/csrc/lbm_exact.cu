@@ -36,8 +36,10 @@ static cudaError_t launch_exact_fm(int kernel, const LaunchArgs& a)
     using M = ModeExact;
     const int grid = grid_for(a.P.n, a.block);
     if (kernel == KERNEL_OBSERVE) {
-        Outputs<double> out{(double*)a.rho, (double*)a.u, a.partials, a.prev_partials, a.prev_count, a.prev_sums};
-        k_observe<M, FM><<<grid, a.block, 0, a.stream>>>(a.P, make_streams<double>(a.src, nullptr, a.P.n), a.post,
+        Outputs<double> out{(double*)a.rho, (double*)a.u, a.partials, a.prev_partials, a.prev_count, a.prev_sums,
+                          a.first, a.count};
+        const int ogrid = a.count < 0 ? grid : grid_for(a.count, a.block);
+        k_observe<M, FM><<<ogrid, a.block, 0, a.stream>>>(a.P, make_streams<double>(a.src, nullptr, a.P.n), a.post,
                                                           a.f_out, out);
         return cudaGetLastError();
     }

@@ -31,8 +31,10 @@ static cudaError_t launch_fast_t(int kernel, const LaunchArgs& a)
     using M = ModeFast<T>;
     const int grid = grid_for(a.P.n, a.block);
     if (kernel == KERNEL_OBSERVE) {
-        Outputs<float> out{(float*)a.rho, (float*)a.u, a.partials, a.prev_partials, a.prev_count, a.prev_sums};
-        k_observe<M, FM><<<grid, a.block, 0, a.stream>>>(a.P, make_streams<T>(a.src, nullptr, a.P.n), a.post,
+        Outputs<float> out{(float*)a.rho, (float*)a.u, a.partials, a.prev_partials, a.prev_count, a.prev_sums,
+                          a.first, a.count};
+        const int ogrid = a.count < 0 ? grid : grid_for(a.count, a.block);
+        k_observe<M, FM><<<ogrid, a.block, 0, a.stream>>>(a.P, make_streams<T>(a.src, nullptr, a.P.n), a.post,
                                                           a.f_out, out);
         return cudaGetLastError();
     }

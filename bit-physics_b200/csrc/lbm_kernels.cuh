@@ -41,6 +41,8 @@ struct Outputs {
     const double* prev_partials = nullptr; // optional: partials of the previous launch on the
     int prev_count = 0;                    // stream (prev_count rows), which block 0 reduces
     double* prev_sums = nullptr;           // into prev_sums (5)
+    int first = 0;                         // k_observe: the window of cells [first,
+    int count = -1;                        // first + count); count < 0: all cells
 };
 
 // Block-level FP64 reduction of 5 values, fixed tree (deterministic for a
@@ -307,16 +309,17 @@ __global__ void __launch_bounds__(256) k_collide_local(Params P, Streams<typenam
 
 // Current state without advancing it: f_n as f64 (optional; used for POST
 // states -- a PRE buffer is read out exactly by k_load_f64), readback and
-// conservation partials.  post = true rebuilds f_n from P_{n-1}; false reads
+// conservation partials, over the cell window of out (default: all cells).  post = true rebuilds f_n from P_{n-1}; false reads
 // the PRE buffer in place.
 template <class M, int FM>
 __global__ void __launch_bounds__(256) k_observe(Params P, Streams<typename M::T> S, bool post,
                                                  double* __restrict__ f_out, Outputs<typename M::C> out)
 {
     using C = typename M::C;
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int end = out.count < 0 ? P.n : out.first + out.count;
+    const int idx = out.first + blockIdx.x * blockDim.x + threadIdx.x;
     double cons[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    if (idx < P.n) {
+    if (idx < end) {
         C f[Q];
         bool solid;
         const int fl = P.has_flags ? (int)P.flags[idx] : 0;

@@ -25,6 +25,8 @@ struct LaunchArgs {
     const double* prev_partials;  // with partials: block 0 also reduces these prev_count rows
     int prev_count;               // (the previous launch's partials) into prev_sums
     double* prev_sums;
+    int first;          // KERNEL_OBSERVE: cell window [first, first + count);
+    int count;          // count < 0: all cells
     int block;
     int vec;            // cells per thread of KERNEL_STEP (1, or 2 for ModeFast with nz even)
     cudaStream_t stream;

@@ -114,6 +114,9 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "lbm_batch_autotune": ([_h, _i, _dp], C.c_int),
     "lbm_batch_synchronize": ([_h], C.c_int),
     "lbm_conservation_noalloc": ([_h, _h, _i, _i, _i, _h, _h], C.c_int),
+    "lbm_plane_get": ([_h, _i, C.c_uint32, _h], C.c_int),
+    "lbm_plane_put": ([_h, _i, C.c_uint32, _h], C.c_int),
+    "lbm_conservation_planes": ([_h, _i, _i, _dp], C.c_int),
     "lbm_get_rho_u_dev": ([_h, _h, _h], C.c_int),
     "lbm_set_porosity_dev": ([_h, _h], C.c_int),
     "lbm_tape_forward": ([_h, _i, _i, C.POINTER(_h)], C.c_int),

@@ -239,6 +239,22 @@ class Lattice:
     def synchronize(self) -> None:
         N.check(N.lib().lbm_synchronize(self._h))
 
+    # -- x-slab planes ---------------------------------------------------------
+    def plane_get_device(self, x: int, dir_mask: int, ptr: int) -> None:
+        """Copy plane x of the stored array, directions in dir_mask, to the
+        device buffer at ptr (popcount * ny * nz storage elements)."""
+        N.check(N.lib().lbm_plane_get(self._h, int(x), int(dir_mask), C.c_void_p(ptr)))
+
+    def plane_put_device(self, x: int, dir_mask: int, ptr: int) -> None:
+        """The reverse of plane_get_device."""
+        N.check(N.lib().lbm_plane_put(self._h, int(x), int(dir_mask), C.c_void_p(ptr)))
+
+    def conservation_planes(self, x0: int, x1: int) -> np.ndarray:
+        """FP64 {sum rho, sum m} over the cells of the x-planes [x0, x1)."""
+        out = np.empty(4)
+        N.check(N.lib().lbm_conservation_planes(self._h, int(x0), int(x1), N.ptr(out)))
+        return out
+
     # -- device pointers and the adjoint tape ----------------------------------
     def rho_u_device(self, rho_ptr: int | None, u_ptr: int | None) -> None:
         """Write rho (n) and u (3, n) as f64 to device addresses (integers,

@@ -1,0 +1,199 @@
+"""x-slab decomposition of one lattice over several engines.
+
+x is the slowest axis of the population arrays, so a slab of x-planes is
+contiguous per direction.  Slab r owns the global planes [x0, x1) and holds
+them in a local lattice of x1 - x0 + 2 planes, periodic in x: local plane 0
+and local plane x1 - x0 + 1 are halo planes.  Before every step that pulls
+(every step after the first one from a set state), and before a readback,
+each slab exchanges one plane per face: the 5 directions with c_x = +1 of its
+last owned plane go to the right neighbour's left halo, the 5 with c_x = -1 of
+its first owned plane to the left neighbour's right halo -- exactly the
+post-collision populations the neighbour's boundary plane pulls.  The halo
+planes' own updates are discarded (overwritten by the next exchange); flags,
+porosity and force fields carry the neighbours' planes so that bounce-back
+masks and forces across a face are those of the global lattice.
+
+Requirements: x periodic globally (inflow / outflow cells are flags and are
+fine), every slab at least 3 planes, and no outflow cell on a slab's first
+owned plane (an outflow cell copies the state of x - 1, which a slab holds
+only from its second plane on).  No counterpart in the reference (it runs on
+one device).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+PLUS_X = (1, 7, 9, 11, 13)     # c_x = +1: pulled across a slab's left face
+MINUS_X = (2, 8, 10, 12, 14)   # c_x = -1: pulled across its right face
+MASK_PLUS = sum(1 << d for d in PLUS_X)
+MASK_MINUS = sum(1 << d for d in MINUS_X)
+CELL_OUTFLOW = 3
+
+
+def slab_bounds(nx: int, parts: int) -> list[tuple[int, int]]:
+    """Contiguous split of [0, nx) into `parts` slabs as even as possible."""
+    if parts < 1 or nx < 3 * parts:
+        raise ValueError(f"cannot split {nx} x-planes into {parts} slabs of at least 3 planes")
+    base, rem = divmod(nx, parts)
+    out, x = [], 0
+    for r in range(parts):
+        w = base + (1 if r < rem else 0)
+        out.append((x, x + w))
+        x += w
+    return out
+
+
+def with_halos(field, x0: int, x1: int, nx: int, axis: int = 0):
+    """Global planes x0 - 1 .. x1 (periodic wrap in x) of a field whose axis
+    `axis` is x."""
+    idx = np.arange(x0 - 1, x1 + 1) % nx
+    return np.take(np.asarray(field), idx, axis=axis)
+
+
+class SlabLattice:
+    """One slab.  `engine` is the local lattice (local shape (x1 - x0 + 2, ny,
+    nz), periodic in x) wrapped by an adapter with plane_get(x, mask) ->
+    buffer, plane_put(x, mask, buffer), step(n), set_populations(f),
+    get_populations(), rho_u(), conservation_planes(x0, x1)."""
+
+    def __init__(self, engine, x0: int, x1: int, flags=None, nx: int | None = None):
+        self.engine = engine
+        self.x0, self.x1 = int(x0), int(x1)
+        self.width = self.x1 - self.x0
+        if self.width < 3:
+            raise ValueError("a slab needs at least 3 planes")
+        if flags is not None and nx is not None:
+            first = np.asarray(flags)[self.x0 % nx] & 3
+            if np.any(first == CELL_OUTFLOW):
+                raise ValueError(f"outflow cells on the first plane (x = {self.x0}) of a slab")
+        self.stepped = False
+
+    # faces -------------------------------------------------------------------
+    def export_faces(self):
+        """(to the left neighbour, to the right neighbour) buffers."""
+        return (self.engine.plane_get(1, MASK_MINUS), self.engine.plane_get(self.width, MASK_PLUS))
+
+    def import_faces(self, from_left, from_right) -> None:
+        self.engine.plane_put(0, MASK_PLUS, from_left)
+        self.engine.plane_put(self.width + 1, MASK_MINUS, from_right)
+
+    # state ---------------------------------------------------------------------
+    def set_populations(self, f_global) -> None:
+        """Set from the global populations (19, nx, ny, nz)."""
+        f = np.asarray(f_global)
+        self.engine.set_populations(with_halos(f, self.x0, self.x1, f.shape[1], axis=1))
+        self.stepped = False
+
+    def owned(self, a, axis: int = 0):
+        sl = [slice(None)] * np.ndim(a)
+        sl[axis] = slice(1, self.width + 1)
+        return a[tuple(sl)]
+
+
+class SlabGroup:
+    """Slabs of one lattice in one process (one device or several): the
+    exchange is a direct copy between the slabs' engines."""
+
+    def __init__(self, slabs: list[SlabLattice]):
+        self.slabs = slabs
+
+    def exchange(self) -> None:
+        faces = [s.export_faces() for s in self.slabs]
+        k = len(self.slabs)
+        for r, s in enumerate(self.slabs):
+            s.import_faces(faces[(r - 1) % k][1], faces[(r + 1) % k][0])
+
+    def step(self, n_steps: int = 1) -> None:
+        for _ in range(int(n_steps)):
+            if self.slabs[0].stepped:
+                self.exchange()
+            for s in self.slabs:
+                s.engine.step(1)
+                s.stepped = True
+
+    def _fresh(self) -> None:
+        if self.slabs[0].stepped:
+            self.exchange()
+
+    def rho_u(self):
+        self._fresh()
+        parts = [s.engine.rho_u() for s in self.slabs]
+        rho = np.concatenate([s.owned(p[0], 0) for s, p in zip(self.slabs, parts, strict=True)], axis=0)
+        u = np.concatenate([s.owned(p[1], 1) for s, p in zip(self.slabs, parts, strict=True)], axis=1)
+        return rho, u
+
+    def get_populations(self):
+        self._fresh()
+        return np.concatenate([s.owned(s.engine.get_populations(), 1) for s in self.slabs], axis=1)
+
+    def conservation(self):
+        self._fresh()
+        return np.sum([s.engine.conservation_planes(1, s.width + 1) for s in self.slabs], axis=0)
+
+
+def exchange_distributed(slab: SlabLattice, rank: int, world: int, to_tensor=None, from_tensor=None) -> None:
+    """The face exchange of one slab per rank with torch.distributed point-to-
+    point operations (NCCL for device tensors, gloo for host tensors); world 1
+    exchanges with itself (periodic x).  to_tensor / from_tensor convert the
+    engine's buffers (identity for torch tensors)."""
+    import torch
+    import torch.distributed as dist
+
+    to_t = to_tensor or (lambda b: b)
+    from_t = from_tensor or (lambda t, like: t)
+    left_send, right_send = slab.export_faces()
+    ls, rs = to_t(left_send), to_t(right_send)
+    if world == 1:
+        slab.import_faces(right_send, left_send)
+        return
+    lr, rr = torch.empty_like(rs), torch.empty_like(ls)
+    right, left = (rank + 1) % world, (rank - 1) % world
+    ops = [dist.P2POp(dist.isend, rs, right), dist.P2POp(dist.irecv, lr, left),
+           dist.P2POp(dist.isend, ls, left), dist.P2POp(dist.irecv, rr, right)]
+    for req in dist.batch_isend_irecv(ops):
+        req.wait()
+    slab.import_faces(from_t(lr, left_send), from_t(rr, right_send))
+
+
+class GpuEngine:
+    """Adapter of a Lattice (local slab shape) to the SlabLattice engine
+    interface: plane buffers are torch device tensors on the lattice's
+    stream (the caller's current torch stream)."""
+
+    _ELEM = {"f64": 8, "f32": 4, "f16": 2, "bf16": 2}
+
+    def __init__(self, lattice, storage: str):
+        import torch
+
+        self.lat = lattice
+        self.torch = torch
+        nx, ny, nz = lattice.shape
+        self.count = 5 * ny * nz * self._ELEM[storage]
+
+    def plane_get(self, x: int, mask: int):
+        buf = self.torch.empty(self.count, dtype=self.torch.uint8, device="cuda")
+        self.lat.plane_get_device(x, mask, buf.data_ptr())
+        return buf
+
+    def plane_put(self, x: int, mask: int, buf) -> None:
+        self.lat.plane_put_device(x, mask, buf.data_ptr())
+
+    def step(self, n: int) -> None:
+        self.lat.step(n)
+
+    def set_populations(self, f) -> None:
+        self.lat.set_populations(f)
+
+    def get_populations(self):
+        return self.lat.get_populations()
+
+    def rho_u(self):
+        return self.lat.rho_u()
+
+    def conservation_planes(self, x0: int, x1: int):
+        return self.lat.conservation_planes(x0, x1)
+
+
+__all__ = ["GpuEngine", "MASK_MINUS", "MASK_PLUS", "MINUS_X", "PLUS_X", "SlabGroup", "SlabLattice",
+           "exchange_distributed", "slab_bounds", "with_halos"]

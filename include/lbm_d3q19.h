@@ -233,6 +233,20 @@ int lbm_get_rho_u_dev(lbm_lattice* h, double* rho, double* u);
 /* lbm_set_porosity from device memory (n floats in [0, 1], checked). */
 int lbm_set_porosity_dev(lbm_lattice* h, const float* alpha);
 
+/* ---- x-slab decomposition --------------------------------------------------
+ * No counterpart in the reference (single-device).  A lattice split in x over
+ * several handles (x-slabs with one halo plane per side, periodic in x)
+ * exchanges, before each step, the populations that cross a slab face: plane
+ * x of the stored array (after a step: the post-collision populations) for
+ * the directions in dir_mask (bit d = direction d), to / from a device buffer
+ * of popcount(dir_mask) * ny * nz storage elements, direction-major in
+ * increasing d.  Enqueued on the lattice's stream. */
+int lbm_plane_get(lbm_lattice* h, int32_t x, uint32_t dir_mask, void* dst);
+int lbm_plane_put(lbm_lattice* h, int32_t x, uint32_t dir_mask, const void* src);
+/* FP64 {sum rho, sum m} over the cells of the x-planes [x0, x1) (a slab's
+ * owned planes); as lbm_conservation otherwise. */
+int lbm_conservation_planes(lbm_lattice* h, int32_t x0, int32_t x1, double* out4);
+
 /* ---- adjoint: gradients through taped steps -------------------------------
  * The differentiable run the reference does not have (its Warp kernels are
  * not taped).  lbm_tape_forward runs n_steps from the lattice's current PRE
