@@ -626,6 +626,76 @@ def run_ensemble(args):
                       / out["per_lattice_launches"]["glups"]}), flush=True)
 
 
+def run_slab(args, rank: int, world: int, local_rank: int):
+    """x-slab strong scaling: the headline sphere channel (256 x 128 x 128)
+    split in x over the ranks, one slab per GPU with a halo plane per side;
+    every step exchanges 5 populations per face with its neighbours (NCCL
+    point-to-point; one rank exchanges with itself).  Value: global cells x
+    steps / (max over ranks of the CUDA-event time)."""
+    import torch
+
+    from lattice_boltzmann_d3q19_b200 import Lattice
+    from lattice_boltzmann_d3q19_b200.slab import GpuEngine, SlabLattice, exchange_distributed, slab_bounds, \
+        with_halos
+
+    dist_on = world > 1
+    if dist_on:
+        torch.distributed.init_process_group("nccl", timeout=timedelta(seconds=300))
+    torch.cuda.set_device(local_rank)
+    storage = args.storage
+    nx = SHAPE[0]
+    flags = channel_geometry()
+    x0, x1 = slab_bounds(nx, world)[rank]
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        lat = Lattice((x1 - x0 + 2, *SHAPE[1:]), TAU, storage=storage, inflow_u=(INFLOW_U, 0.0, 0.0),
+                      device=local_rank)
+        lat.set_stream(stream.cuda_stream)
+        lat.set_flags(with_halos(flags, x0, x1, nx))
+        lat.set_equilibrium(1.0, (INFLOW_U, 0.0, 0.0))
+        slab = SlabLattice(GpuEngine(lat, storage), x0, x1, flags=flags, nx=nx)
+
+        def advance(k):
+            for _ in range(k):
+                if slab.stepped:
+                    exchange_distributed(slab, rank, world)
+                lat.step(1)
+                slab.stepped = True
+
+        advance(args.warmup)
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        if dist_on:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        start.record(stream)
+        advance(args.steps)
+        end.record(stream)
+        torch.cuda.synchronize()
+        if dist_on:
+            torch.distributed.barrier()
+        ms = start.elapsed_time(end)
+        healthy = lat.check_health()
+        lat.close()
+    ms_max = ms
+    if dist_on:
+        t = torch.tensor([ms], device=f"cuda:{local_rank}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_max = float(t.item())
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    n = int(np.prod(SHAPE))
+    elem = {"f64": 8, "f32": 4, "f16": 2, "bf16": 2}[storage]
+    print(json.dumps({
+        "metric": "D3Q19 GLUPS, x-slab decomposition of one lattice", "workload": "slab", "unit": "GLUPS",
+        "value": n * args.steps / (ms_max / 1e3) / 1e9, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "scaling": "strong", "dtype": storage,
+        "healthy": healthy, "halo_bytes_per_face_per_step": 5 * SHAPE[1] * SHAPE[2] * elem,
+        "config": {"workload": WORKLOAD, "slabs": world, "planes_per_slab": x1 - x0},
+    }), flush=True)
+
+
 ADJ_STEPS, ADJ_EVERY = 2000, 50
 
 
@@ -755,7 +825,7 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cells-per-thread", type=int, default=0, choices=[0, 1, 2])
     ap.add_argument("--staging", default="auto", choices=["auto", "registers", "tma"])
-    ap.add_argument("--workload", default="channel", choices=["channel", "cavity", "sweep", "ensemble", "adjoint"])
+    ap.add_argument("--workload", default="channel", choices=["channel", "cavity", "sweep", "ensemble", "adjoint", "slab"])
     args = ap.parse_args()
     global CELLS_PER_THREAD, STAGING
     CELLS_PER_THREAD = args.cells_per_thread
@@ -767,6 +837,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.workload == "slab":
+        run_slab(args, rank, world, local_rank)
         return
     if args.workload != "channel":
         {"cavity": run_cavity, "sweep": run_sweep, "ensemble": run_ensemble,
