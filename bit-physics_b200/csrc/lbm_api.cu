@@ -843,16 +843,9 @@ static int plane_copy(lbm_lattice* h, int32_t x, uint32_t dir_mask, void* dev, b
     if (dir_mask == 0 || dir_mask >= (1u << Q)) return fail(LBM_ERR_INVALID, "direction mask 0x%x invalid", dir_mask);
     if ((rc = check_device_ptr(h, dev, "plane buffer"))) return rc;
     const size_t plane = (size_t)h->desc.ny * h->desc.nz * h->elem;
-    char* base = (char*)h->buf[h->cur];
-    char* buf = (char*)dev;
-    size_t k = 0;
-    for (int d = 0; d < Q; ++d) {
-        if (!((dir_mask >> d) & 1u)) continue;
-        char* st = base + ((size_t)d * h->n + (size_t)x * h->desc.ny * h->desc.nz) * h->elem;
-        if (get) CK(cudaMemcpyAsync(buf + k * plane, st, plane, cudaMemcpyDeviceToDevice, h->stream), "plane copy");
-        else CK(cudaMemcpyAsync(st, buf + k * plane, plane, cudaMemcpyDeviceToDevice, h->stream), "plane copy");
-        ++k;
-    }
+    CK(launch_plane_copy(h->buf[h->cur], (size_t)h->n * h->elem, (size_t)x * plane, plane, dir_mask, dev, get,
+                         h->stream),
+       "plane copy");
     return LBM_OK;
 }
 

@@ -189,6 +189,51 @@ __global__ void k_reduce_partials(const double* __restrict__ partials, int nbloc
     block_sum5(v, out5);
 }
 
+// Plane copies of the x-slab exchange: blockIdx.y picks the k-th direction of
+// the mask (dirs[k]); each thread moves words of W bytes between the plane of
+// that direction in the stored array and slot k of the packed buffer.
+struct PlaneDirs {
+    int d[Q];
+};
+
+template <class W>
+__global__ void k_plane_copy(char* __restrict__ base, size_t dir_stride, size_t plane_off, size_t words,
+                             PlaneDirs dirs, char* __restrict__ buf, bool get)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= words) return;
+    const int k = blockIdx.y;
+    W* plane = reinterpret_cast<W*>(base + (size_t)dirs.d[k] * dir_stride + plane_off);
+    W* slot = reinterpret_cast<W*>(buf) + (size_t)k * words;
+    if (get) slot[i] = plane[i];
+    else plane[i] = slot[i];
+}
+
+cudaError_t launch_plane_copy(void* base, size_t dir_stride, size_t plane_off, size_t plane_bytes, uint32_t mask,
+                              void* buf, bool get, cudaStream_t s)
+{
+    PlaneDirs dirs{};
+    int count = 0;
+    for (int d = 0; d < Q; ++d)
+        if ((mask >> d) & 1u) dirs.d[count++] = d;
+    if (count == 0) return cudaErrorInvalidValue;
+    const int block = 256;
+    // 16-byte words when every plane, slot and the buffer are 16-byte aligned
+    const bool wide = plane_bytes % 16 == 0 && dir_stride % 16 == 0 && plane_off % 16 == 0 &&
+                      reinterpret_cast<uintptr_t>(base) % 16 == 0 && reinterpret_cast<uintptr_t>(buf) % 16 == 0;
+    if (wide) {
+        const size_t words = plane_bytes / 16;
+        const dim3 grid((unsigned)((words + block - 1) / block), (unsigned)count);
+        k_plane_copy<uint4><<<grid, block, 0, s>>>((char*)base, dir_stride, plane_off, words, dirs, (char*)buf, get);
+    } else {
+        const size_t words = plane_bytes / 2;  // every storage element is a multiple of 2 bytes
+        const dim3 grid((unsigned)((words + block - 1) / block), (unsigned)count);
+        k_plane_copy<unsigned short><<<grid, block, 0, s>>>((char*)base, dir_stride, plane_off, words, dirs,
+                                                            (char*)buf, get);
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t launch_reduce_partials(const double* partials, int nblocks, double* out5, cudaStream_t s)
 {
     k_reduce_partials<<<1, 256, 0, s>>>(partials, nblocks, out5);

@@ -50,6 +50,11 @@ cudaError_t launch_feq_init(int storage, const Params& P, const double* rho, con
                             cudaStream_t s);
 cudaError_t launch_mark_near_solid(const Params& P, uint8_t* flags, uint32_t* bbmask, cudaStream_t s);
 cudaError_t launch_reduce_partials(const double* partials, int nblocks, double* out5, cudaStream_t s);
+// x-slab exchange: plane (plane_off bytes into each direction, plane_bytes
+// long, directions dir_stride bytes apart) of the directions in mask to
+// (get) or from the packed buffer, one launch.
+cudaError_t launch_plane_copy(void* base, size_t dir_stride, size_t plane_off, size_t plane_bytes, uint32_t mask,
+                              void* buf, bool get, cudaStream_t s);
 
 // Batched step (one launch for many lattices): records and items in device
 // memory, see lbm_batch.cuh.  `records` points to BatchLattice<T> for the
