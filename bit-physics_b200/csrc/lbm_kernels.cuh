@@ -171,7 +171,8 @@ __global__ void __launch_bounds__(256) k_step(Params P, Streams<typename M::T> S
 // resolved one at a time with the scalar resolve_state.
 template <class M, int FM, int OUT>
 __device__ __forceinline__ void step_pair(const Params& P, const Streams<typename M::T>& S,
-                                          const Outputs<typename M::C>& out, int idx0, double* cons)
+                                          const Outputs<typename M::C>& out, int idx0, double* cons,
+                                          bool live = true)
 {
     using T = typename M::T;
     int x, y, z0;
@@ -216,13 +217,13 @@ __device__ __forceinline__ void step_pair(const Params& P, const Streams<typenam
         emit<M, FM, OUT_RHO_U>(P, out, idx0 + 1, !fluid1, f, cons);
     }
     const auto mo = M::template collide2<FM>(P, idx0, h, [&](int d, float2 v) {
-        st_dev2(S.dst[d] + idx0, d, fluid0 ? v.x : M::solid(P, d), fluid1 ? v.y : M::solid(P, d));
+        if (live) st_dev2(S.dst[d] + idx0, d, fluid0 ? v.x : M::solid(P, d), fluid1 ? v.y : M::solid(P, d));
     });
     if constexpr ((OUT & OUT_SUMS) != 0) {
         // the collision's own pre-collision moments (density deviation,
         // momentum), assigned: the caller's sums hold this pair only, so they
         // are not live during the step
-        const double k0 = fluid0 ? 1.0 : 0.0, k1 = fluid1 ? 1.0 : 0.0;
+        const double k0 = live && fluid0 ? 1.0 : 0.0, k1 = live && fluid1 ? 1.0 : 0.0;
         cons[0] = k0 * (double)mo.rd.x + k1 * (double)mo.rd.y;
         cons[1] = k0 * (double)mo.mx.x + k1 * (double)mo.mx.y;
         cons[2] = k0 * (double)mo.my.x + k1 * (double)mo.my.y;
@@ -271,8 +272,17 @@ __global__ void __launch_bounds__(256, LBM_STEP2_MIN_BLOCKS) k_step2(Params P, S
     if constexpr ((OUT & OUT_SUMS) != 0) reduce_prev(out);
     const int idx0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
     double cons[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    if (idx0 < P.n) step_pair<M, FM, OUT>(P, S, out, idx0, cons);
-    if constexpr ((OUT & OUT_SUMS) != 0) block_sum5(cons, out.partials + (size_t)blockIdx.x * 5);
+    if constexpr ((OUT & OUT_SUMS) != 0) {
+        // Threads past the end compute the last pair again, store nothing and
+        // add nothing: a step with no branch around it and a block reduction
+        // after it keeps the register allocation of the plain kernel (a
+        // guarded step followed by the reduction spilled ~3x as many bytes).
+        const bool live = idx0 < P.n;
+        step_pair<M, FM, OUT>(P, S, out, live ? idx0 : P.n - 2, cons, live);
+        block_sum5(cons, out.partials + (size_t)blockIdx.x * 5);
+    } else {
+        if (idx0 < P.n) step_pair<M, FM, OUT>(P, S, out, idx0, cons);
+    }
 }
 
 // Step from PRE for one cell: read f_n in place, collide, write P_n.
