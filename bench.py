@@ -172,6 +172,8 @@ def step_kernel(storage: str) -> str:
     """Name of the step kernel a lattice of the headline shape runs."""
     if STAGING == "tma" and storage != "f64":
         return f"k_step_tma<{storage}>"
+    if STAGING in ("pipelined", "auto") and storage in ("f16", "bf16") and CELLS_PER_THREAD in (0, 2):
+        return f"k_step2_pipe<{storage}>"  # the headline lattice has ~28 pairs per thread
     cpt = CELLS_PER_THREAD or (1 if storage == "f64" else 2)
     return f"{'k_step2' if cpt == 2 else 'k_step'}<{storage}>"
 
@@ -179,8 +181,11 @@ def step_kernel(storage: str) -> str:
 def make_lattice(storage: str, flags, device: int):
     from lattice_boltzmann_d3q19_b200 import Lattice
 
-    # the TMA-staged kernel serves the f32-arithmetic storages only
-    staging = STAGING if storage != "f64" else "auto"
+    # the TMA-staged kernel serves the f32-arithmetic storages, the pipelined
+    # one the 16-bit storages
+    staging = STAGING
+    if storage == "f64" or (STAGING == "pipelined" and storage not in ("f16", "bf16")):
+        staging = "auto"
     lat = Lattice(SHAPE, TAU, storage=storage, inflow_u=(INFLOW_U, 0.0, 0.0), device=device,
                   cells_per_thread=CELLS_PER_THREAD, staging=staging)
     lat.set_flags(flags)
@@ -824,7 +829,7 @@ def main():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cells-per-thread", type=int, default=0, choices=[0, 1, 2])
-    ap.add_argument("--staging", default="auto", choices=["auto", "registers", "tma"])
+    ap.add_argument("--staging", default="auto", choices=["auto", "registers", "tma", "pipelined"])
     ap.add_argument("--workload", default="channel", choices=["channel", "cavity", "sweep", "ensemble", "adjoint", "slab"])
     args = ap.parse_args()
     global CELLS_PER_THREAD, STAGING

@@ -249,7 +249,7 @@ __device__ __forceinline__ double cell_lambda(const Params& P, const AdjIO<typen
     } else {
         const Nbr nb = make_nbr(P, x, y, z);
         const int fl = P.has_flags ? (int)P.flags[c] : 0;
-        const uint32_t bb = (fl & FLAG_NEAR_SOLID) ? P.bbmask[c] : 0u;
+        const uint32_t bb = (fl & FLAG_NEAR_SOLID) ? P.bbmask[c] & CW_MASK_BITS : 0u;
         adj_pull<typename M::C>(P, io.Lin, nb, c, x, y, z, bb, lam);
         return adj_collide<M, FM>(P, c, mo, lam);
     }
@@ -382,7 +382,7 @@ __global__ void __launch_bounds__(128) k_adjoint_special(Params P, Streams<typen
         return;
     }
     const bool face = on_walled_face(P, x, y, z);
-    const uint32_t bb = (fl & FLAG_NEAR_SOLID) ? P.bbmask[idx] : 0u;
+    const uint32_t bb = (fl & FLAG_NEAR_SOLID) ? P.bbmask[idx] & CW_MASK_BITS : 0u;
     if (type == CELL_OUTFLOW) {
         // own state came from x - 1; the x + 1 outflow cell copies B_x(g(x))
         gather<M>(S, nb, f);

@@ -170,6 +170,8 @@ cudaError_t lbm::api::launch(lbm_lattice* h, int kernel, const void* src, void* 
     a.stream = h->stream;
     a.grid_used = grid_used;
     a.tma_grid = 0;
+    a.pipe_grid = kernel == KERNEL_STEP ? h->pipe_grid : 0;
+    a.sums_grid = kernel == KERNEL_STEP ? h->sums_grid : 0;
     if (kernel == KERNEL_STEP && h->use_tma) {
         a.tma_grid = h->tma_grid;
         a.tile = h->tile;
@@ -305,8 +307,8 @@ int lbm_create(const lbm_desc* desc, lbm_lattice** out)
         return fail(LBM_ERR_INVALID, "block_size must be 0 or a multiple of 32 in [32, 256]");
     if (desc->cells_per_thread < 0 || desc->cells_per_thread > 2)
         return fail(LBM_ERR_INVALID, "cells_per_thread must be 0 (auto), 1 or 2");
-    if (desc->staging < LBM_STAGING_AUTO || desc->staging > LBM_STAGING_TMA)
-        return fail(LBM_ERR_INVALID, "staging must be LBM_STAGING_AUTO, _REGISTERS or _TMA");
+    if (desc->staging < LBM_STAGING_AUTO || desc->staging > LBM_STAGING_PIPELINED)
+        return fail(LBM_ERR_INVALID, "staging must be LBM_STAGING_AUTO, _REGISTERS, _TMA or _PIPELINED");
     if (desc->cells_per_thread == 2 && (desc->storage == LBM_STORAGE_F64 || desc->nz % 2 != 0))
         return fail(LBM_ERR_UNSUPPORTED, "cells_per_thread = 2 needs f32/f16/bf16 storage and an even nz");
     int ndev = lbm_device_count();
@@ -357,11 +359,36 @@ int lbm_create(const lbm_desc* desc, lbm_lattice** out)
             h->tma_grid = grid;
         }
     }
+    // Pipelined two-cell step (the default for 16-bit storage on lattices
+    // with at least 4 pairs per thread of its resident grid): on the
+    // 256x128x128 sphere channel f16 58 GLUPS against 55 for k_step2 (64-68
+    // against 60-63 without obstacles); on a 64^3 box (1.7 pairs per thread,
+    // half the threads idle in the last round) slower than k_step2.
+    const bool pipe_ok = (h->storage == LBM_STORAGE_F16_SHIFT || h->storage == LBM_STORAGE_BF16_SHIFT) && h->vec == 2;
+    if (desc->staging == LBM_STAGING_PIPELINED && !pipe_ok)
+        return cleanup(fail(LBM_ERR_UNSUPPORTED, "pipelined staging needs f16/bf16 storage, two cells per "
+                                                 "thread and an even nz"));
+    if (pipe_ok && (desc->staging == LBM_STAGING_PIPELINED || desc->staging == LBM_STAGING_AUTO)) {
+        const int grid = pipe_grid_fast(h->storage, desc->force_mode, h->block);
+        if (grid <= 0) return cleanup(fail(LBM_ERR_CUDA, "pipelined step: no resident blocks"));
+        const long long pairs = (long long)h->n / 2, threads = (long long)grid * h->block;
+        if (desc->staging == LBM_STAGING_PIPELINED || pairs >= 4 * threads) h->pipe_grid = grid;
+    }
+    // Steps with FP64 sums (two cells per thread) run one block per resident
+    // slot, each thread looping over pairs: one partial row per block.
+    if (h->storage != LBM_STORAGE_F64 && h->vec == 2) {
+        h->sums_grid = sums_grid_fast(h->storage, desc->force_mode, h->block);
+        if (h->sums_grid <= 0) return cleanup(fail(LBM_ERR_CUDA, "step with sums: no resident blocks"));
+    }
     if (desc->staging == LBM_STAGING_TMA && !h->use_tma)
         return cleanup(fail(LBM_ERR_UNSUPPORTED, "TMA staging needs f32/f16/bf16 storage, two cells per thread, "
                                                  "an even nz and nz * element size a multiple of 16 bytes"));
+    // Room for the partial rows of any launch: one per block of a per-cell
+    // grid, of the TMA grid or of the resident sums grid (which exceeds the
+    // per-cell grid on small lattices).
     h->partial_blocks = grid_for(h->n, h->block);
     if (h->partial_blocks < h->tma_grid) h->partial_blocks = h->tma_grid;
+    if (h->partial_blocks < h->sums_grid) h->partial_blocks = h->sums_grid;
     e = cudaMalloc((void**)&h->partials, sizeof(double) * 2 * 5 * (size_t)h->partial_blocks);
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->sums, sizeof(double) * 5);
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->err, sizeof(int));
@@ -788,7 +815,8 @@ int lbm_conservation(lbm_lattice* h, double* out4)
     if ((rc = check_force_ready(h))) return rc;
     cudaError_t e = launch(h, KERNEL_OBSERVE, h->buf[h->cur], nullptr, !h->pre, nullptr, nullptr, nullptr, h->partials);
     if (e != cudaSuccess) return cuda_fail(e, "conservation kernel");
-    CK(launch_reduce_partials(h->partials, h->partial_blocks, h->sums, h->stream), "partial reduction");
+    // the rows the observe launch wrote (one per block of its per-cell grid)
+    CK(launch_reduce_partials(h->partials, grid_for(h->n, h->block), h->sums, h->stream), "partial reduction");
     double s[5];
     CK(cudaMemcpyAsync(s, h->sums, sizeof(s), cudaMemcpyDeviceToHost, h->stream), "sum copy");
     CK(cudaStreamSynchronize(h->stream), "sum sync");

@@ -28,6 +28,12 @@ enum CellType : int { CELL_FLUID = 0, CELL_SOLID = 1, CELL_INFLOW = 2, CELL_OUTF
 // Internal flag bit: the cell has a solid cell among its 18 pull sources
 // (its bounce-back mask is nonzero).
 constexpr int FLAG_NEAR_SOLID = 0x80;
+// Per-cell 32-bit cell word (Params::bbmask): bits 1..18 the bounce-back
+// mask (bit d: the pull source of direction d is solid), bits 24..31 the
+// cell's flag byte (type and FLAG_NEAR_SOLID), so that one load gives a
+// step kernel both.
+constexpr int CW_FLAG_SHIFT = 24;
+constexpr uint32_t CW_MASK_BITS = 0x7fffeu;
 enum ForceMode : int { FORCE_NONE = 0, FORCE_UNIFORM = 1, FORCE_FIELD = 2, FORCE_DRAG = 3 };
 enum Face : int { FACE_XM = 0, FACE_XP = 1, FACE_YM = 2, FACE_YP = 3, FACE_ZM = 4, FACE_ZP = 5 };
 
@@ -84,7 +90,7 @@ struct Params {
     int wall_sum_pairwise; // nx * nz == 1 (see ModeExact::rho_wall)
     int* err;              // device error word (pipeline wait timeouts), may be null
     const uint8_t* flags;
-    const uint32_t* bbmask; // (n): bit d set when the pull source of d is solid
+    const uint32_t* bbmask; // (n) cell words: bounce-back mask | flag byte << CW_FLAG_SHIFT
     const void* force; // (3, n): double for ModeExact, float for ModeFast
     const float* porosity;
     // f64 values (ModeExact), all host-computed with the reference's expressions
@@ -742,11 +748,11 @@ __device__ __forceinline__ bool resolve_state(const Params& P, const Streams<typ
         const Nbr nb2 = make_nbr(P, gx, y, z);
         gather<M>(S, nb2, f);
         const bool face2 = on_walled_face(P, gx, y, z);
-        const uint32_t m = (g & FLAG_NEAR_SOLID) ? P.bbmask[gidx] : 0u;
+        const uint32_t m = (g & FLAG_NEAR_SOLID) ? P.bbmask[gidx] & CW_MASK_BITS : 0u;
         if (face2 || m) boundary_fix<M>(P, S, nb2, gx, y, z, gidx, face2, m, f);
         return true;
     }
-    const uint32_t m = (fl & FLAG_NEAR_SOLID) ? P.bbmask[idx] : 0u;
+    const uint32_t m = (fl & FLAG_NEAR_SOLID) ? P.bbmask[idx] & CW_MASK_BITS : 0u;
     boundary_fix<M>(P, S, nb, x, y, z, idx, face, m, f);
     return true;
 }

@@ -167,10 +167,11 @@ __global__ void k_mark_near_solid(Params P, uint8_t* __restrict__ flags, uint32_
         for (int d = 1; d < Q; ++d)
             if ((flags[nb.src(d)] & 3) == CELL_SOLID) mask |= 1u << d;
     }
-    bbmask[idx] = mask;
+    const int fl = type | (mask ? FLAG_NEAR_SOLID : 0);
+    bbmask[idx] = mask | ((uint32_t)fl << CW_FLAG_SHIFT);
     // Every thread reads only the low bits of its neighbours, so writing the
     // high bit in place is race-free.
-    flags[idx] = (uint8_t)(type | (mask ? FLAG_NEAR_SOLID : 0));
+    flags[idx] = (uint8_t)fl;
 }
 
 cudaError_t launch_mark_near_solid(const Params& P, uint8_t* flags, uint32_t* bbmask, cudaStream_t s)

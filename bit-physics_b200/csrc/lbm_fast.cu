@@ -12,6 +12,20 @@ static void launch_step_out(int kernel, const LaunchArgs& a, int grid)
     using T = typename M::T;
     Outputs<float> out{(float*)a.rho, (float*)a.u, a.partials, a.prev_partials, a.prev_count, a.prev_sums};
     const Streams<T> S = make_streams<T>(a.src, a.dst, a.P.n);
+    if constexpr (sizeof(T) == 2 && OUT == OUT_NONE) {
+        if (kernel == KERNEL_STEP && a.vec == 2 && a.pipe_grid > 0) {
+            k_step2_pipe<M, FM><<<a.pipe_grid, a.block, 0, a.stream>>>(a.P, S);
+            if (a.grid_used) *a.grid_used = a.pipe_grid;
+            return;
+        }
+    }
+    if constexpr (OUT == OUT_SUMS) {
+        if (kernel == KERNEL_STEP && a.vec == 2 && a.sums_grid > 0) {
+            k_step2_sums<M, FM><<<a.sums_grid, a.block, 0, a.stream>>>(a.P, S, out);
+            if (a.grid_used) *a.grid_used = a.sums_grid;
+            return;
+        }
+    }
     if (kernel == KERNEL_STEP && a.vec == 2) {
         const int grid2 = grid_for(a.P.n / 2, a.block);
         k_step2<M, FM, OUT><<<grid2, a.block, 0, a.stream>>>(a.P, S, out);
@@ -134,6 +148,51 @@ size_t batch_record_bytes(int storage)
     default: return 0;
     }
 }
+
+// Resident blocks per SM x SMs of the current device for a kernel.
+template <class K>
+static int resident_grid(K kernel, int block)
+{
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) != cudaSuccess) return 0;
+    return sms * per_sm;
+}
+
+template <class T, int FM>
+static int loop_grid_t(bool sums, int block)
+{
+    if (sums) return resident_grid(k_step2_sums<ModeFast<T>, FM>, block);
+    if constexpr (sizeof(T) == 2) return resident_grid(k_step2_pipe<ModeFast<T>, FM>, block);
+    return 0;
+}
+
+template <class T>
+static int loop_grid_fm(bool sums, int force_mode, int block)
+{
+    switch (force_mode) {
+    case FORCE_NONE: return loop_grid_t<T, FORCE_NONE>(sums, block);
+    case FORCE_UNIFORM: return loop_grid_t<T, FORCE_UNIFORM>(sums, block);
+    case FORCE_FIELD: return loop_grid_t<T, FORCE_FIELD>(sums, block);
+    case FORCE_DRAG: return loop_grid_t<T, FORCE_DRAG>(sums, block);
+    default: return 0;
+    }
+}
+
+static int loop_grid(bool sums, int storage, int force_mode, int block)
+{
+    switch (storage) {
+    case STORAGE_F32: return loop_grid_fm<float>(sums, force_mode, block);
+    case STORAGE_F16: return loop_grid_fm<__half>(sums, force_mode, block);
+    case STORAGE_BF16: return loop_grid_fm<__nv_bfloat16>(sums, force_mode, block);
+    default: return 0;
+    }
+}
+
+int pipe_grid_fast(int storage, int force_mode, int block) { return loop_grid(false, storage, force_mode, block); }
+
+int sums_grid_fast(int storage, int force_mode, int block) { return loop_grid(true, storage, force_mode, block); }
 
 cudaError_t launch_fast(int storage, int kernel, int force_mode, const LaunchArgs& a)
 {

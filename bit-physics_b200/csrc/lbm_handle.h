@@ -44,6 +44,8 @@ struct lbm_lattice {
     int graph_version = -1;
     bool use_tma = false;
     int tma_grid = 0;
+    int pipe_grid = 0;  // > 0: steps without outputs run k_step2_pipe
+    int sums_grid = 0;  // > 0: steps with FP64 sums run k_step2_sums
     lbm::TileCfg tile{};
     lbm::Params P{};
 };

@@ -16,6 +16,14 @@
 #ifndef LBM_STEP2_MIN_BLOCKS
 #define LBM_STEP2_MIN_BLOCKS 3
 #endif
+// Which two-cell step kernels read the 32-bit cell words (flag byte and
+// bounce-back mask in one load) instead of the flag bytes: 0 none, 1 the
+// 16-bit storages, 2 all.  Measured on the 256x128x128 sphere channel: f32
+// 36.2 GLUPS with cell words against 39.0 with flag bytes (4 B per cell
+// read instead of 1); f16 / bf16 equal or faster.
+#ifndef LBM_CELL_WORD
+#define LBM_CELL_WORD 1
+#endif
 
 namespace lbm {
 
@@ -161,6 +169,54 @@ __global__ void __launch_bounds__(256) k_step(Params P, Streams<typename M::T> S
     if constexpr ((OUT & OUT_SUMS) != 0) block_sum5(cons, out.partials + (size_t)blockIdx.x * 5);
 }
 
+// Boundary rules of a pair (cells idx0, idx0 + 1 of one row) after the
+// speculative own-position gather h.  The common case -- neither cell on a
+// walled face nor an inflow / outflow cell, i.e. fluid or solid cells, some
+// next to a solid -- is resolved for both cells at once: their bounce-back
+// masks (passed in with CW, else one 8-byte load), then all half-way
+// bounce-back loads of both cells in one batch, instead of the per-cell
+// resolve_state one cell after the other (two dependent memory latencies per
+// cell).  Everything else goes through resolve_state per cell.
+template <bool CW>
+struct PairMasks {
+    uint32_t m0 = 0u, m1 = 0u;  // with CW: the cells' masks (zero for solid cells)
+};
+
+template <class M, bool CW>
+__device__ __forceinline__ void resolve_pair(const Params& P, const Streams<typename M::T>& S, int idx0, int x,
+                                             int y, int z0, int fl0, int fl1, bool face, const Nbr& nb0, int zp1,
+                                             float2* h, bool& fluid0, bool& fluid1, PairMasks<CW> cm = {})
+{
+    const int t0 = fl0 & 3, t1 = fl1 & 3;
+    const bool plain0 = t0 == CELL_FLUID || t0 == CELL_SOLID, plain1 = t1 == CELL_FLUID || t1 == CELL_SOLID;
+    if (!face && plain0 && plain1) {
+        fluid0 = t0 == CELL_FLUID;
+        fluid1 = t1 == CELL_FLUID;
+        const bool near0 = fluid0 && (fl0 & FLAG_NEAR_SOLID), near1 = fluid1 && (fl1 & FLAG_NEAR_SOLID);
+        if (near0 || near1) {
+            uint32_t m0 = cm.m0, m1 = cm.m1;
+            if constexpr (!CW) {
+                const uint2 mm = __ldg(reinterpret_cast<const uint2*>(P.bbmask + idx0));
+                m0 = near0 ? mm.x & CW_MASK_BITS : 0u;
+                m1 = near1 ? mm.y & CW_MASK_BITS : 0u;
+            }
+#pragma unroll
+            for (int d = 1; d < Q; ++d) {
+                const int o = opp(d);
+                if ((m0 >> d) & 1u) h[d].x = M::load(S.src[o] + idx0, o);
+                if ((m1 >> d) & 1u) h[d].y = M::load(S.src[o] + idx0 + 1, o);
+            }
+        }
+        return;
+    }
+    fluid0 = resolve_state<M>(P, S, idx0, x, y, z0, fl0, nb0, Lane<0>{h});
+    Nbr nb1 = nb0;
+    nb1.Z[0] = z0;
+    nb1.Z[1] = z0 + 1;
+    nb1.Z[2] = zp1;
+    fluid1 = resolve_state<M>(P, S, idx0 + 1, x, y, z0 + 1, fl1, nb1, Lane<1>{h});
+}
+
 // Fused step from POST, two z-adjacent cells (z0 even, z0 + 1) per thread, for
 // the f32-arithmetic storages; requires nz even (both cells share a row, rows
 // start at even indices).  Both cells' values of a direction live in one
@@ -175,13 +231,23 @@ __device__ __forceinline__ void step_pair(const Params& P, const Streams<typenam
                                           bool live = true)
 {
     using T = typename M::T;
+    constexpr bool CW = LBM_CELL_WORD >= 2 || (LBM_CELL_WORD >= 1 && sizeof(T) == 2);
     int x, y, z0;
     decode_xyz(P, idx0, x, y, z0);
     int fl0 = 0, fl1 = 0;
+    PairMasks<CW> cm;
     if (P.has_flags) {
-        const unsigned short both = __ldg(reinterpret_cast<const unsigned short*>(P.flags + idx0));
-        fl0 = both & 0xff;
-        fl1 = both >> 8;
+        if constexpr (CW) {
+            const uint2 w = __ldg(reinterpret_cast<const uint2*>(P.bbmask + idx0));
+            fl0 = (int)(w.x >> CW_FLAG_SHIFT);
+            fl1 = (int)(w.y >> CW_FLAG_SHIFT);
+            cm.m0 = w.x & CW_MASK_BITS;
+            cm.m1 = w.y & CW_MASK_BITS;
+        } else {
+            const unsigned short both = __ldg(reinterpret_cast<const unsigned short*>(P.flags + idx0));
+            fl0 = both & 0xff;
+            fl1 = both >> 8;
+        }
     }
     const Nbr nb0 = make_nbr(P, x, y, z0);
     const int zp1 = z0 + 2 == P.nz ? 0 : z0 + 2; // (z0 + 1) + 1, wrapped
@@ -199,14 +265,8 @@ __device__ __forceinline__ void step_pair(const Params& P, const Streams<typenam
     }
     bool fluid0 = true, fluid1 = true;
     const bool face = on_walled_face(P, x, y, z0) || on_walled_face(P, x, y, z0 + 1);
-    if ((fl0 | fl1 | (int)face) != 0) {
-        fluid0 = resolve_state<M>(P, S, idx0, x, y, z0, fl0, nb0, Lane<0>{h});
-        Nbr nb1 = nb0;
-        nb1.Z[0] = z0;
-        nb1.Z[1] = z0 + 1;
-        nb1.Z[2] = zp1;
-        fluid1 = resolve_state<M>(P, S, idx0 + 1, x, y, z0 + 1, fl1, nb1, Lane<1>{h});
-    }
+    if ((fl0 | fl1 | (int)face) != 0)
+        resolve_pair<M, CW>(P, S, idx0, x, y, z0, fl0, fl1, face, nb0, zp1, h, fluid0, fluid1, cm);
     if constexpr ((OUT & OUT_RHO_U) != 0) {
         float f[Q];
 #pragma unroll
@@ -282,6 +342,142 @@ __global__ void __launch_bounds__(256, LBM_STEP2_MIN_BLOCKS) k_step2(Params P, S
         block_sum5(cons, out.partials + (size_t)blockIdx.x * 5);
     } else {
         if (idx0 < P.n) step_pair<M, FM, OUT>(P, S, out, idx0, cons);
+    }
+}
+
+// k_step2 with the FP64 conservation sums over a grid of resident blocks: each
+// thread steps pairs p, p + G, p + 2G, ... (G threads in the grid) and adds
+// their moments in f64 registers; one block reduction per block and launch
+// instead of one per 256 pairs, and no block barrier between pairs.  Every
+// thread runs the same number of iterations (threads past the end recompute
+// the last pair and store and add nothing), so no branch surrounds a step.
+// The per-thread sums follow a fixed order: results are deterministic for a
+// given grid.
+template <class M, int FM>
+__global__ void __launch_bounds__(256, LBM_STEP2_MIN_BLOCKS) k_step2_sums(Params P, Streams<typename M::T> S,
+                                                                         Outputs<typename M::C> out)
+{
+    reduce_prev(out);
+    const int np = P.n >> 1;
+    const int stride = gridDim.x * blockDim.x;
+    const int iters = (np + stride - 1) / stride;
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int it = 0; it < iters; ++it, p += stride) {
+        const bool live = p < np;
+        double cons[5];
+        step_pair<M, FM, OUT_SUMS>(P, S, out, live ? 2 * p : P.n - 2, cons, live);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) acc[k] += cons[k];
+    }
+    block_sum5(acc, out.partials + (size_t)blockIdx.x * 5);
+}
+
+// ---------------------------------------------------------------------------
+// Software-pipelined two-cell step for 16-bit storage
+// ---------------------------------------------------------------------------
+
+// Raw pulled values of one pair as they come from memory: the c_z = 0
+// directions as one aligned 32-bit word (both cells), the z-shifted ones as
+// two 16-bit values, and the pair's cell words; kept unconverted so that the
+// loads stay in flight while the previous pair is collided.
+struct Raw16 {
+    uint32_t w[Q];
+    unsigned short a[Q], b[Q];
+    uint32_t cw0, cw1;  // 0 without flags
+};
+
+__device__ __forceinline__ float2 word_dev2(uint32_t w, __half)
+{
+    __half2 v;
+    memcpy(&v, &w, sizeof v);
+    return __half22float2(v);
+}
+__device__ __forceinline__ float2 word_dev2(uint32_t w, __nv_bfloat16)
+{
+    // bfloat16 is the upper half of a binary32: widening is a shift
+    return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xffff0000u));
+}
+__device__ __forceinline__ float half_dev(unsigned short v, __half) { return __half2float(__ushort_as_half(v)); }
+__device__ __forceinline__ float half_dev(unsigned short v, __nv_bfloat16)
+{
+    return __uint_as_float((uint32_t)v << 16);
+}
+
+// Issue the loads of pair idx0 (the plain pull gather of step_pair and the
+// pair's cell words); nothing waits for them here.
+template <class T>
+__device__ __forceinline__ void fetch_pair16(const Params& P, const Streams<T>& S, int idx0, Raw16& r)
+{
+    int x, y, z0;
+    decode_xyz(P, idx0, x, y, z0);
+    r.cw0 = r.cw1 = 0u;
+    if (P.has_flags) {
+        const uint2 cw = __ldg(reinterpret_cast<const uint2*>(P.bbmask + idx0));
+        r.cw0 = cw.x;
+        r.cw1 = cw.y;
+    }
+    const Nbr nb0 = make_nbr(P, x, y, z0);
+    const int zp1 = z0 + 2 == P.nz ? 0 : z0 + 2;
+#pragma unroll
+    for (int d = 0; d < Q; ++d) {
+        const unsigned short* p =
+            reinterpret_cast<const unsigned short*>(S.src[d]) + nb0.X[1 - cx(d)] + nb0.Y[1 - cy(d)];
+        if (cz(d) == 0) {
+            r.w[d] = __ldg(reinterpret_cast<const unsigned int*>(p + z0));
+        } else if (cz(d) == 1) {
+            r.a[d] = __ldg(p + nb0.Z[0]);
+            r.b[d] = __ldg(p + z0);
+        } else {
+            r.a[d] = __ldg(p + z0 + 1);
+            r.b[d] = __ldg(p + zp1);
+        }
+    }
+}
+
+// The two-cell step of k_step2 (no outputs) over a grid-stride loop of
+// pairs, with the next pair's gather issued before this pair's boundary
+// rules, collision and stores, so that every warp keeps a pair of loads in
+// flight through its arithmetic.  For f16 / bf16 storage, whose 76 B of loads
+// per pair do not cover the HBM latency at k_step2's occupancy.  128
+// registers, two blocks of 256 per SM.
+template <class M, int FM>
+__global__ void __launch_bounds__(256, 2) k_step2_pipe(Params P, Streams<typename M::T> S)
+{
+    using T = typename M::T;
+    static_assert(sizeof(T) == 2, "k_step2_pipe: 16-bit storage only");
+    const int np = P.n >> 1;
+    const int stride = gridDim.x * blockDim.x;
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    Raw16 r;
+    fetch_pair16(P, S, 2 * p, r);
+    for (;;) {
+        const int idx0 = 2 * p;
+        float2 h[Q];
+#pragma unroll
+        for (int d = 0; d < Q; ++d)
+            h[d] = cz(d) == 0 ? word_dev2(r.w[d], T{}) : make_float2(half_dev(r.a[d], T{}), half_dev(r.b[d], T{}));
+        const int fl0 = (int)(r.cw0 >> CW_FLAG_SHIFT), fl1 = (int)(r.cw1 >> CW_FLAG_SHIFT);
+        PairMasks<true> cm;
+        cm.m0 = r.cw0 & CW_MASK_BITS;
+        cm.m1 = r.cw1 & CW_MASK_BITS;
+        const int q = p + stride;
+        if (q < np) fetch_pair16(P, S, 2 * q, r);
+        int x, y, z0;
+        decode_xyz(P, idx0, x, y, z0);
+        bool fluid0 = true, fluid1 = true;
+        const bool face = on_walled_face(P, x, y, z0) || on_walled_face(P, x, y, z0 + 1);
+        if ((fl0 | fl1 | (int)face) != 0) {
+            const Nbr nb0 = make_nbr(P, x, y, z0);
+            const int zp1 = z0 + 2 == P.nz ? 0 : z0 + 2;
+            resolve_pair<M, true>(P, S, idx0, x, y, z0, fl0, fl1, face, nb0, zp1, h, fluid0, fluid1, cm);
+        }
+        M::template collide2<FM>(P, idx0, h, [&](int d, float2 v) {
+            st_dev2(S.dst[d] + idx0, d, fluid0 ? v.x : M::solid(P, d), fluid1 ? v.y : M::solid(P, d));
+        });
+        if (q >= np) break;
+        p = q;
     }
 }
 

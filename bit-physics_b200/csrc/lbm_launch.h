@@ -33,6 +33,10 @@ struct LaunchArgs {
     int* grid_used;     // optional: receives the launched grid size (partial rows written)
     int tma_grid;       // > 0: KERNEL_STEP runs the TMA-staged kernel with this grid
     TileCfg tile;
+    int pipe_grid = 0;  // > 0: a 16-bit two-cell KERNEL_STEP without outputs runs
+                        // k_step2_pipe with this grid
+    int sums_grid = 0;  // > 0: a two-cell KERNEL_STEP with partials runs
+                        // k_step2_sums with this grid
 };
 
 // Output selection of a step launch (OUT_* bits of lbm_kernels.cuh) from the
@@ -44,6 +48,12 @@ inline int grid_for(long long work, int block) { return (int)((work + block - 1)
 // Stateful engine kernels.
 cudaError_t launch_exact(int kernel, int force_mode, const LaunchArgs& a);
 cudaError_t launch_fast(int storage, int kernel, int force_mode, const LaunchArgs& a);
+// Grids of the grid-stride two-cell kernels for this storage / force model /
+// block size on the current device (resident blocks per SM x SMs); 0 where
+// the kernel does not apply.  k_step2_pipe: f16 / bf16; k_step2_sums: f32 /
+// f16 / bf16.
+int pipe_grid_fast(int storage, int force_mode, int block);
+int sums_grid_fast(int storage, int force_mode, int block);
 cudaError_t launch_store_f64(int storage, const Params& P, const double* f, void* dst, cudaStream_t s);
 cudaError_t launch_load_f64(int storage, const Params& P, const void* src, double* f, cudaStream_t s);
 cudaError_t launch_feq_init(int storage, const Params& P, const double* rho, const double* u, void* dst,

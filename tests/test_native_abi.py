@@ -49,7 +49,7 @@ def test_desc_layout_matches_header():
 @pytest.mark.parametrize(
     "field,value",
     [("nx", 0), ("storage", 9), ("force_mode", 7), ("tau", 0.5), ("periodic", 8), ("block_size", 48),
-     ("cells_per_thread", 3), ("staging", 3)],
+     ("cells_per_thread", 3), ("staging", 4)],
 )
 def test_create_rejects_bad_descriptors(field, value):
     d = N.LbmDesc()
