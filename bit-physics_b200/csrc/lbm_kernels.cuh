@@ -16,6 +16,12 @@
 #ifndef LBM_STEP2_MIN_BLOCKS
 #define LBM_STEP2_MIN_BLOCKS 3
 #endif
+// k_step2_sums at 2 blocks of 256 per SM (128 registers, no spills) against
+// 3 (80 registers, 204 B of spill stores): steps with FP64 sums, f32 sphere
+// channel, 34.5 against 32.2 GLUPS.
+#ifndef LBM_SUMS_MIN_BLOCKS
+#define LBM_SUMS_MIN_BLOCKS 2
+#endif
 // Which two-cell step kernels read the 32-bit cell words (flag byte and
 // bounce-back mask in one load) instead of the flag bytes: 0 none, 1 the
 // 16-bit storages, 2 all.  Measured on the 256x128x128 sphere channel: f32
@@ -169,6 +175,26 @@ __global__ void __launch_bounds__(256) k_step(Params P, Streams<typename M::T> S
     if constexpr ((OUT & OUT_SUMS) != 0) block_sum5(cons, out.partials + (size_t)blockIdx.x * 5);
 }
 
+// Plain pull gather of the pair (x, y, z0), (x, y, z0 + 1) described by nb
+// (zp1 = z0 + 2, wrapped): the c_z = 0 directions as one vector load.
+template <class M>
+__device__ __forceinline__ void gather_pair(const Streams<typename M::T>& S, const Nbr& nb, int z0, int zp1,
+                                            float2* h)
+{
+    using T = typename M::T;
+#pragma unroll
+    for (int d = 0; d < Q; ++d) {
+        const T* p = S.src[d] + nb.X[1 - cx(d)] + nb.Y[1 - cy(d)];
+        if (cz(d) == 0) {
+            ld_dev2(p + z0, d, h[d].x, h[d].y);
+        } else if (cz(d) == 1) {
+            h[d] = ld_dev_pair(p + nb.Z[0], p + z0, d);
+        } else {
+            h[d] = ld_dev_pair(p + z0 + 1, p + zp1, d);
+        }
+    }
+}
+
 // Boundary rules of a pair (cells idx0, idx0 + 1 of one row) after the
 // speculative own-position gather h.  The common case -- neither cell on a
 // walled face nor an inflow / outflow cell, i.e. fluid or solid cells, some
@@ -208,6 +234,25 @@ __device__ __forceinline__ void resolve_pair(const Params& P, const Streams<type
             }
         }
         return;
+    }
+    // Two outflow cells whose x - 1 neighbours are plain fluid cells (the
+    // common case: the outflow plane of a channel): one pair gather at x - 1,
+    // as resolve_state does per cell.  f32 storage only: sphere channel
+    // 38.9 -> 39.1 GLUPS (inflow / outflow planes only: 40.1 -> 40.8), while
+    // the 16-bit kernels compiled with it ran 2-10 % slower even on lattices
+    // without flags.
+    if (sizeof(typename M::T) == 4 && !face && t0 == CELL_OUTFLOW && t1 == CELL_OUTFLOW) {
+        const int gx = x == 0 ? P.nx - 1 : x - 1;
+        const int gidx0 = idx0 + (gx - x) * P.nynz;
+        const unsigned short gb = __ldg(reinterpret_cast<const unsigned short*>(P.flags + gidx0));
+        int g0 = gb & 0xff, g1 = gb >> 8;
+        if ((g0 & 3) == CELL_OUTFLOW) g0 &= ~3;
+        if ((g1 & 3) == CELL_OUTFLOW) g1 &= ~3;
+        if ((g0 | g1) == 0 && !on_walled_face(P, gx, y, z0) && !on_walled_face(P, gx, y, z0 + 1)) {
+            gather_pair<M>(S, make_nbr(P, gx, y, z0), z0, zp1, h);
+            fluid0 = fluid1 = true;
+            return;
+        }
     }
     fluid0 = resolve_state<M>(P, S, idx0, x, y, z0, fl0, nb0, Lane<0>{h});
     Nbr nb1 = nb0;
@@ -252,17 +297,7 @@ __device__ __forceinline__ void step_pair(const Params& P, const Streams<typenam
     const Nbr nb0 = make_nbr(P, x, y, z0);
     const int zp1 = z0 + 2 == P.nz ? 0 : z0 + 2; // (z0 + 1) + 1, wrapped
     float2 h[Q];
-#pragma unroll
-    for (int d = 0; d < Q; ++d) {
-        const T* p = S.src[d] + nb0.X[1 - cx(d)] + nb0.Y[1 - cy(d)];
-        if (cz(d) == 0) {
-            ld_dev2(p + z0, d, h[d].x, h[d].y);
-        } else if (cz(d) == 1) {
-            h[d] = ld_dev_pair(p + nb0.Z[0], p + z0, d);
-        } else {
-            h[d] = ld_dev_pair(p + z0 + 1, p + zp1, d);
-        }
-    }
+    gather_pair<M>(S, nb0, z0, zp1, h);
     bool fluid0 = true, fluid1 = true;
     const bool face = on_walled_face(P, x, y, z0) || on_walled_face(P, x, y, z0 + 1);
     if ((fl0 | fl1 | (int)face) != 0)
@@ -354,7 +389,7 @@ __global__ void __launch_bounds__(256, LBM_STEP2_MIN_BLOCKS) k_step2(Params P, S
 // The per-thread sums follow a fixed order: results are deterministic for a
 // given grid.
 template <class M, int FM>
-__global__ void __launch_bounds__(256, LBM_STEP2_MIN_BLOCKS) k_step2_sums(Params P, Streams<typename M::T> S,
+__global__ void __launch_bounds__(256, LBM_SUMS_MIN_BLOCKS) k_step2_sums(Params P, Streams<typename M::T> S,
                                                                          Outputs<typename M::C> out)
 {
     reduce_prev(out);

@@ -285,6 +285,40 @@ def test_pipelined_staging_bit_identical_to_registers(storage, case):
         assert np.array_equal(outs["pipelined"][k], outs["registers"][k]), k
 
 
+@pytest.mark.parametrize("storage", ["f16", "bf16"])
+@pytest.mark.parametrize("force_mode", ["field", "drag"])
+def test_pipelined_staging_per_cell_forces_bit_identical(storage, force_mode):
+    """Per-cell force inputs (an f32 force field; porosity drag) read as
+    (cell, cell + 1) pairs by the pipelined kernel, against the
+    register-staged two-cell kernel."""
+    from lattice_boltzmann_d3q19_b200 import geometry
+
+    shape = (24, 10, 12)
+    flags = np.zeros(shape, dtype=np.uint8)
+    flags[0] = 2
+    flags[-1] = 3
+    flags[12, 3:6, 4:8] = 1
+    force = 1e-5 * np.random.default_rng(5).standard_normal((3, *shape))
+    alpha = geometry.smooth_porosity(shape, sigma=2.0, seed=9)
+    f0 = random_state(shape, 95, amp=0.01)
+    outs = {}
+    for staging in ("pipelined", "registers"):
+        kw = {"drag_k": 0.05, "body_force": (1e-6, 0.0, 0.0)} if force_mode == "drag" else {}
+        lat = Lattice(shape, 0.7, storage=storage, force_mode=force_mode, inflow_u=(0.03, 0.0, 0.0),
+                      staging=staging, cells_per_thread=2, **kw)
+        with lat:
+            lat.set_flags(flags)
+            if force_mode == "drag":
+                lat.set_porosity(alpha)
+            else:
+                lat.set_force_field(force)
+            lat.set_populations(f0)
+            lat.step(1)
+            lat.step(20)
+            outs[staging] = lat.get_populations()
+    assert np.array_equal(outs["pipelined"], outs["registers"])
+
+
 def test_pipelined_staging_covers_many_pairs_per_thread():
     """Several pairs per thread of the resident grid (the prefetch carried
     across loop iterations), against the register-staged kernel."""
