@@ -321,10 +321,10 @@ int lbm_create(const lbm_desc* desc, lbm_lattice** out)
     h->storage = desc->storage;
     h->n = desc->nx * desc->ny * desc->nz;
     h->elem = storage_bytes(desc->storage);
-    // 128-thread blocks for the f32-arithmetic storages: on the 256x128x128
-    // sphere channel f32 39.5 against 38.9 GLUPS with 256, f16 (pipelined)
-    // 59.1 against 58.4 (192: 38.7 / 52.4).
-    h->block = desc->block_size ? desc->block_size : (desc->storage == LBM_STORAGE_F64 ? 256 : 128);
+    // 128-thread blocks: on the 256x128x128 sphere channel f32 39.5 against
+    // 38.9 GLUPS with 256, f16 (pipelined) 59.1 against 58.4 (192: 38.7 /
+    // 52.4), f64 17.1 against 16.5.
+    h->block = desc->block_size ? desc->block_size : 128;
     // Two cells per thread (packed f32x2 arithmetic) cuts the instructions
     // per cell; measured on the 256x128x128 sphere channel: f16 41 -> 50
     // GLUPS, f32 unchanged (bandwidth-bound).  Needs an even nz.

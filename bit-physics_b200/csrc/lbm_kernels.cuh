@@ -165,8 +165,12 @@ __device__ __forceinline__ void step_single(const Params& P, const Streams<typen
     }
 }
 
+// One cell per thread (f64 storage; odd-nz f32-arithmetic lattices).  At 3
+// blocks of 256 per SM the f64 kernel runs in 80 registers (93 unbounded,
+// 2 blocks): 17.1 against 14.5 GLUPS on the 256x128x128 sphere channel with
+// 128-thread blocks; f64 results do not depend on it (no contraction).
 template <class M, int FM, int OUT>
-__global__ void __launch_bounds__(256) k_step(Params P, Streams<typename M::T> S, Outputs<typename M::C> out)
+__global__ void __launch_bounds__(256, 3) k_step(Params P, Streams<typename M::T> S, Outputs<typename M::C> out)
 {
     if constexpr ((OUT & OUT_SUMS) != 0) reduce_prev(out);
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
