@@ -5,6 +5,11 @@
 #include "lbm_adjoint.cuh"
 #include "lbm_launch.h"
 
+// Threads per block of the per-cell adjoint level kernels.
+#ifndef LBM_ADJ_BLOCK
+#define LBM_ADJ_BLOCK 128
+#endif
+
 namespace lbm {
 
 __global__ void k_widen(const float* __restrict__ in, double* __restrict__ out, size_t count)
@@ -38,7 +43,7 @@ cudaError_t launch_level_m(int level, const AdjointArgs& a)
     using C = typename M::C;
     AdjIO<C> io{(const C*)a.Lin, (C*)a.Lout, a.grad_rho, a.grad_u, a.dalpha, a.grad_f0};
     const Streams<T> S = make_streams<T>(a.src, nullptr, a.P.n);
-    const int block = 256;
+    const int block = LBM_ADJ_BLOCK;
     const int grid = grid_for(a.P.n, block);
     const int sb = 128, sg = grid_for(a.n_special, sb);
     cudaStream_t ss = a.special_stream ? a.special_stream : a.stream;
