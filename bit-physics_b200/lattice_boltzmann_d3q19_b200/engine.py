@@ -195,9 +195,20 @@ class Lattice:
     def step_count(self) -> int:
         return int(N.lib().lbm_step_count(self._h))
 
-    def rho_u(self) -> tuple[np.ndarray, np.ndarray]:
-        rho = np.empty(self.shape)
-        u = np.empty((3, *self.shape))
+    def rho_u(self, out: tuple[np.ndarray, np.ndarray] | None = None) -> tuple[np.ndarray, np.ndarray]:
+        """Density (nx, ny, nz) and velocity (3, nx, ny, nz) as f64 host arrays.
+        ``out``: caller-owned (rho, u) arrays to fill instead (C-contiguous
+        float64 of those shapes), e.g. views of pinned memory, which the
+        device-to-host copy then fills at full speed."""
+        if out is None:
+            rho = np.empty(self.shape)
+            u = np.empty((3, *self.shape))
+        else:
+            rho, u = out
+            for a, shape, name in ((rho, self.shape, "rho"), (u, (3, *self.shape), "u")):
+                if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.shape == shape
+                        and a.flags.c_contiguous and a.flags.writeable):
+                    raise ValueError(f"out {name} must be a writeable C-contiguous float64 array of shape {shape}")
         N.check(N.lib().lbm_get_rho_u(self._h, N.ptr(rho), N.ptr(u)))
         return rho, u
 

@@ -445,3 +445,21 @@ def test_many_handles_and_stream():
         assert np.allclose(u[0], 0.01, atol=1e-3)
         lat.close()
     assert N.lib().lbm_set_stream(C.c_void_p(), None) == N.LBM_ERR_INVALID
+
+
+def test_rho_u_into_caller_arrays():
+    """rho_u(out=...) fills caller-owned arrays with the values rho_u()
+    returns, and rejects arrays of the wrong shape, type or layout."""
+    shape = (8, 6, 10)
+    lat = Lattice(shape, 0.7, storage="f16", inflow_u=(0.03, 0.0, 0.0))
+    with lat:
+        lat.set_populations(random_state(shape, 97, amp=0.01))
+        lat.step(3)
+        rho, u = lat.rho_u()
+        ro, uo = np.full(shape, np.nan), np.full((3, *shape), np.nan)
+        r2, u2 = lat.rho_u(out=(ro, uo))
+        assert r2 is ro and u2 is uo
+        assert np.array_equal(ro, rho) and np.array_equal(uo, u)
+        for bad in ((np.empty(shape, np.float32), uo), (ro, np.empty((3, *shape))[:, ::-1]), (ro, np.empty(shape))):
+            with pytest.raises(ValueError):
+                lat.rho_u(out=bad)
