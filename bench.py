@@ -172,8 +172,8 @@ def step_kernel(storage: str) -> str:
     """Name of the step kernel a lattice of the headline shape runs."""
     if STAGING == "tma" and storage != "f64":
         return f"k_step_tma<{storage}>"
-    if STAGING in ("pipelined", "auto") and storage in ("f16", "bf16") and CELLS_PER_THREAD in (0, 2):
-        return f"k_step2_pipe<{storage}>"  # the headline lattice has ~28 pairs per thread
+    if STAGING == "pipelined" and storage in ("f16", "bf16") and CELLS_PER_THREAD in (0, 2):
+        return f"k_step2_pipe<{storage}>"
     cpt = CELLS_PER_THREAD or (1 if storage == "f64" else 2)
     return f"{'k_step2' if cpt == 2 else 'k_step'}<{storage}>"
 

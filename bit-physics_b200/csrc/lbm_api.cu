@@ -390,20 +390,16 @@ int lbm_create(const lbm_desc* desc, lbm_lattice** out)
             h->tma_grid = grid;
         }
     }
-    // Pipelined two-cell step (the default for 16-bit storage on lattices
-    // with at least 4 pairs per thread of its resident grid): on the
-    // 256x128x128 sphere channel f16 58 GLUPS against 55 for k_step2 (64-68
-    // against 60-63 without obstacles); on a 64^3 box (1.7 pairs per thread,
-    // half the threads idle in the last round) slower than k_step2.
+    // Pipelined two-cell step (on request): on the 256x128x128 sphere channel
+    // f16 58.6-59.1 GLUPS against 60.5-60.7 for k_step2 in 128-thread blocks
+    // at 96 registers, which is therefore the default.
     const bool pipe_ok = (h->storage == LBM_STORAGE_F16_SHIFT || h->storage == LBM_STORAGE_BF16_SHIFT) && h->vec == 2;
     if (desc->staging == LBM_STAGING_PIPELINED && !pipe_ok)
         return cleanup(fail(LBM_ERR_UNSUPPORTED, "pipelined staging needs f16/bf16 storage, two cells per "
                                                  "thread and an even nz"));
-    if (pipe_ok && (desc->staging == LBM_STAGING_PIPELINED || desc->staging == LBM_STAGING_AUTO)) {
-        const int grid = pipe_grid_fast(h->storage, desc->force_mode, h->block);
-        if (grid <= 0) return cleanup(fail(LBM_ERR_CUDA, "pipelined step: no resident blocks"));
-        const long long pairs = (long long)h->n / 2, threads = (long long)grid * h->block;
-        if (desc->staging == LBM_STAGING_PIPELINED || pairs >= 4 * threads) h->pipe_grid = grid;
+    if (desc->staging == LBM_STAGING_PIPELINED) {
+        h->pipe_grid = pipe_grid_fast(h->storage, desc->force_mode, h->block);
+        if (h->pipe_grid <= 0) return cleanup(fail(LBM_ERR_CUDA, "pipelined step: no resident blocks"));
     }
     // Steps with FP64 sums (two cells per thread) run one block per resident
     // slot, each thread looping over pairs: one partial row per block.

@@ -27,8 +27,10 @@ static void launch_step_out(int kernel, const LaunchArgs& a, int grid)
         }
     }
     if (kernel == KERNEL_STEP && a.vec == 2) {
-        const int grid2 = grid_for(a.P.n / 2, a.block);
-        k_step2<M, FM, OUT><<<grid2, a.block, 0, a.stream>>>(a.P, S, out);
+        // at most the kernel's bound (128 threads for 16-bit storage)
+        const int block = a.block < Step2Bounds<T>::threads ? a.block : Step2Bounds<T>::threads;
+        const int grid2 = grid_for(a.P.n / 2, block);
+        k_step2<M, FM, OUT><<<grid2, block, 0, a.stream>>>(a.P, S, out);
         if (a.grid_used) *a.grid_used = grid2;
         return;
     }

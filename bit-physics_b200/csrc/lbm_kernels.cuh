@@ -364,8 +364,26 @@ __device__ __forceinline__ void step_pair_scalar(const Params& P, const Streams<
     });
 }
 
+// Launch bounds of k_step2: f32 storage at 3 blocks of 256 per SM (80
+// registers); the 16-bit storages at 5 blocks of 128 (96 registers, 20
+// warps: f16 sphere channel 60.4 against 59.1 GLUPS at 80 registers and
+// 54.6 at 128; f32 at 96 registers ran 38.1 against 40.1).
+template <class T>
+struct Step2Bounds {
+    static constexpr int threads = 256, blocks = LBM_STEP2_MIN_BLOCKS;
+};
+template <>
+struct Step2Bounds<__half> {
+    static constexpr int threads = 128, blocks = 5;
+};
+template <>
+struct Step2Bounds<__nv_bfloat16> {
+    static constexpr int threads = 128, blocks = 5;
+};
+
 template <class M, int FM, int OUT>
-__global__ void __launch_bounds__(256, LBM_STEP2_MIN_BLOCKS) k_step2(Params P, Streams<typename M::T> S,
+__global__ void __launch_bounds__(Step2Bounds<typename M::T>::threads, Step2Bounds<typename M::T>::blocks)
+    k_step2(Params P, Streams<typename M::T> S,
                                                                     Outputs<typename M::C> out)
 {
     if constexpr ((OUT & OUT_SUMS) != 0) reduce_prev(out);

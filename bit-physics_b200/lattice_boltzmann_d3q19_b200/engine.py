@@ -18,8 +18,8 @@ Beyond the reference (project semantics, pinned to the CPU oracle):
   weights (f16 / bf16, "shift" storage) with f32 arithmetic;
 * ``staging`` / ``cells_per_thread``: which step kernel runs (register-
   staged one or two cells per thread, the software-pipelined two-cell kernel
-  that is the default for f16 / bf16, or TMA shared-memory staging); they
-  change speed, not semantics.
+  for f16 / bf16, or TMA shared-memory staging); they change speed, not
+  semantics.
 """
 
 from __future__ import annotations

@@ -89,9 +89,7 @@ typedef struct lbm_desc {
 } lbm_desc;
 
 /* Step-kernel staging (lbm_desc.staging). */
-#define LBM_STAGING_AUTO 0      /* the fastest measured: pipelined for f16/bf16
-                                   with two cells per thread and >= 4 pairs per
-                                   thread of its resident grid, else registers    */
+#define LBM_STAGING_AUTO 0      /* the fastest measured: registers               */
 #define LBM_STAGING_REGISTERS 1 /* loads straight into registers                  */
 #define LBM_STAGING_TMA 2       /* TMA bulk copies into a shared-memory ring: two
                                    cells per thread, f32/f16/bf16 storage, nz even
