@@ -157,6 +157,48 @@ class ClockSampler:
         }
 
 
+class NvmlClock:
+    """Fast in-process SM-clock sampler (NVML, ~1 ms period) for the short
+    timed repeats that nvidia-smi's 100 ms rows cannot resolve.  samples()
+    returns the SM clocks (MHz) read between two perf_counter instants."""
+
+    def __init__(self, uuid: str | None, device_index: int):
+        self.rows: list[tuple[float, int]] = []
+        self.on = False
+        self.stop_flag = False
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            # NVML numbers GPUs physically; the UUID names the one torch uses
+            self.h = (pynvml.nvmlDeviceGetHandleByUUID(uuid) if uuid
+                      else pynvml.nvmlDeviceGetHandleByIndex(device_index))
+        except Exception:
+            self.nv = None
+            return
+        self.thread = threading.Thread(target=self._run, daemon=True)
+        self.thread.start()
+
+    def _run(self):
+        while not self.stop_flag:
+            if self.on:
+                try:
+                    mhz = self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM)
+                    self.rows.append((time.perf_counter(), int(mhz)))
+                except Exception:
+                    pass
+                time.sleep(0.001)
+            else:
+                time.sleep(0.005)
+
+    def samples(self, t0: float, t1: float) -> list[int]:
+        return [m for (t, m) in list(self.rows) if t0 <= t <= t1]
+
+    def stop(self):
+        self.stop_flag = True
+
+
 def channel_geometry():
     from lattice_boltzmann_d3q19_b200 import geometry
 
@@ -250,21 +292,155 @@ def run_reference(args, rank: int):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+REPEATS = 5          # timed repeats of the requested step count per arm
+PRECISION_STEPS = 5000
+PRECISION_TAUS = (0.51, 0.56, 0.8)
+
+
 def timed_steps(lat, steps: int, stream, torch, dist_on: bool):
+    """One timed region: exactly `steps` steps bracketed by a barrier and a
+    device synchronisation on both sides; CUDA events on the launching stream."""
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
     if dist_on:
         torch.distributed.barrier()
     torch.cuda.synchronize()
     t0 = time.time()
+    p0 = time.perf_counter()
     start.record(stream)
     lat.step(steps)
     end.record(stream)
     torch.cuda.synchronize()
     t1 = time.time()
+    p1 = time.perf_counter()
     if dist_on:
         torch.distributed.barrier()
-    return start.elapsed_time(end), t0, t1
+    return start.elapsed_time(end), t0, t1, p0, p1
+
+
+def timed_repeats(lat, steps: int, repeats: int, stream, torch, dist_on: bool, nvml):
+    """`repeats` timed regions of `steps` steps each; per repeat its device
+    milliseconds, wall interval and the median SM clock NVML saw inside it."""
+    if nvml is not None:
+        nvml.on = True
+    reps = []
+    for _ in range(repeats):
+        ms, t0, t1, p0, p1 = timed_steps(lat, steps, stream, torch, dist_on)
+        mhz = nvml.samples(p0, p1) if nvml is not None else []
+        reps.append({"ms": ms, "t0": t0, "t1": t1,
+                     "sm_mhz": statistics.median(mhz) if mhz else None, "clock_samples": len(mhz)})
+    if nvml is not None:
+        nvml.on = False
+    return reps
+
+
+def median_ms(reps) -> float:
+    return statistics.median(r["ms"] for r in reps)
+
+
+def public_reps(reps):
+    return [{"ms": r["ms"], "sm_mhz": r["sm_mhz"], "clock_samples": r["clock_samples"]} for r in reps]
+
+
+def precision_leg(torch, shape_name: str, dev: int):
+    """Velocity / density error of each storage against the f64 build of the
+    same kernels after PRECISION_STEPS steps from the inflow equilibrium, at
+    tau in PRECISION_TAUS, plus the FP64 mass change of each run.  Errors over
+    fluid cells, computed on the device: u L2-relative (norm of the error
+    field over norm of the f64 field) and max-relative (max error magnitude
+    over max f64 speed); rho L2-relative and max-abs."""
+    from lattice_boltzmann_d3q19_b200 import Lattice
+
+    shape = {"c3": (512, 256, 256), "c2": SHAPE}[shape_name]
+    flags = channel_flags(shape, shape[0] / SHAPE[0])
+    n = int(np.prod(shape))
+    fluid = torch.from_numpy(flags != 1).to(f"cuda:{dev}")
+    stream = torch.cuda.Stream(device=dev)
+    out = {"steps": PRECISION_STEPS, "shape": list(shape),
+           "geometry": "sphere channel" + (" scaled x2 (radii U[8,20])" if shape_name == "c3" else ""),
+           "reference": "f64 GPU build of the same kernels, same steps", "taus": {}}
+    for tau in PRECISION_TAUS:
+        row, ref = {}, None
+        for storage in ("f64", "f32", "f16", "bf16"):
+            lat = Lattice(shape, tau, storage=storage, inflow_u=(INFLOW_U, 0.0, 0.0), device=dev)
+            lat.set_stream(stream.cuda_stream)
+            lat.set_flags(flags)
+            lat.set_equilibrium(1.0, (INFLOW_U, 0.0, 0.0))
+            m0 = lat.conservation()[0]
+            ms = _device_time(lambda: lat.step(PRECISION_STEPS), torch, stream)
+            m1 = lat.conservation()[0]
+            healthy = lat.check_health()
+            rho = torch.empty(shape, dtype=torch.float64, device=f"cuda:{dev}")
+            u = torch.empty((3, *shape), dtype=torch.float64, device=f"cuda:{dev}")
+            lat.rho_u_device(rho.data_ptr(), u.data_ptr())
+            torch.cuda.synchronize()
+            lat.close()
+            entry = {"glups": n * PRECISION_STEPS / (ms / 1e3) / 1e9, "healthy": healthy,
+                     "mass_change_rel": float((m1 - m0) / m0)}
+            if storage == "f64":
+                ref = (rho, u)
+            else:
+                rr, ur = ref
+                du = (u - ur)[:, fluid]
+                urf = ur[:, fluid]
+                dmag = torch.sqrt((du * du).sum(0))
+                umax = torch.sqrt((urf * urf).sum(0)).max()
+                dr = (rho - rr)[fluid]
+                entry.update({
+                    "u_err_l2_rel": float(torch.linalg.vector_norm(du) / torch.linalg.vector_norm(urf)),
+                    "u_err_max_rel": float(dmag.max() / umax),
+                    "rho_err_l2_rel": float(torch.linalg.vector_norm(dr) / torch.linalg.vector_norm(rr[fluid])),
+                    "rho_err_max_abs": float(dr.abs().max()),
+                })
+                del du, urf, dmag, dr
+            row[storage] = entry
+            del rho, u
+        del ref
+        out["taus"][str(tau)] = row
+    return out
+
+
+def adjoint_leg(torch, dev: int):
+    """Backward / forward time of the 128^3 FP32 porosity-drag channel over
+    2000 steps with checkpoints every 50 steps (the adjoint workload's
+    timing, without its gradient check)."""
+    from lattice_boltzmann_d3q19_b200 import geometry
+
+    shape = adjoint_shape()
+    steps = int(os.environ.get("LBM_ADJ_STEPS", ADJ_STEPS))
+    alpha = geometry.smooth_porosity(shape, sigma=4.0, seed=SEED)
+    stream = torch.cuda.Stream(device=dev)
+    box = (3 * shape[0] // 4, shape[0])
+    with torch.cuda.stream(stream):
+        lat = adjoint_lattice("f32", alpha)
+        lat.set_stream(stream.cuda_stream)
+        lat.set_equilibrium()
+        lat.step(3)
+        lat.set_equilibrium()
+        t_fwd = _device_time(lambda: lat.step(steps), torch, stream)
+        lat.set_equilibrium()
+        holder = {}
+        t_tape = _device_time(lambda: holder.update(tape=lat.tape(steps, ADJ_EVERY)), torch, stream)
+        tape = holder["tape"]
+        rho = torch.empty(shape, dtype=torch.float64, device="cuda")
+        u = torch.empty((3, *shape), dtype=torch.float64, device="cuda")
+        lat.rho_u_device(rho.data_ptr(), u.data_ptr())
+        r = rho.clone().requires_grad_(True)
+        v = u.clone().requires_grad_(True)
+        x0, x1 = box
+        L = 0.5 * (r[x0:x1] * (v[:, x0:x1] ** 2).sum(0)).sum()
+        L.backward()
+        ga = torch.empty(shape, dtype=torch.float64, device="cuda")
+        t_bwd = _device_time(lambda: tape.backward(r.grad.data_ptr(), v.grad.data_ptr(), ga.data_ptr()), torch,
+                             stream)
+        finite = bool(torch.isfinite(ga).all())
+        nbytes = tape.nbytes
+        tape.close()
+        lat.close()
+    return {"value": t_bwd / t_fwd, "forward_ms": t_fwd, "taped_forward_ms": t_tape, "backward_ms": t_bwd,
+            "tape_gb": nbytes / 1e9, "gradient_finite": finite,
+            "config": f"{shape[0]}x{shape[1]}x{shape[2]} drag channel, f32, {steps} steps, checkpoints every "
+                      f"{ADJ_EVERY}; backward = segment recompute + adjoint kernels"}
 
 
 def run_ours(args, rank: int, world: int, local_rank: int):
@@ -284,33 +460,30 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     flags = channel_geometry()
     stream = torch.cuda.Stream(device=dev)
     sampler = ClockSampler(dev_id)
+    nvml = NvmlClock(dev_id, dev)
+    if nvml.nv is None:
+        nvml = None
     hbm, hbm_kind = peak_hbm()
+    repeats = max(1, args.repeats)
 
-    def measure(storage: str, steps: int, warmup: int):
+    def measure(storage: str, steps: int, warmup: int, sync_ranks: bool):
         lat = make_lattice(storage, flags, dev)
         lat.set_stream(stream.cuda_stream)
         lat.step(warmup)
-        ms, t0, t1 = timed_steps(lat, steps, stream, torch, False)
-        if not lat.check_health():
-            raise RuntimeError(f"{storage}: non-finite state after {warmup + steps} steps")
-        rho, u = lat.rho_u()
+        reps = timed_repeats(lat, steps, repeats, stream, torch, sync_ranks, nvml)
+        healthy = lat.check_health()
         lat.close()
-        return ms, t0, t1, rho, u
+        return reps, healthy
 
     # headline arm (f32), timed across ranks
-    lat = make_lattice(args.storage, flags, dev)
-    lat.set_stream(stream.cuda_stream)
-    lat.step(args.warmup)
-    ms, t0, t1 = timed_steps(lat, args.steps, stream, torch, dist_on)
-    healthy = lat.check_health()
-    rho_h, u_h = lat.rho_u()
-    lat.close()
+    reps, healthy = measure(args.storage, args.steps, args.warmup, dist_on)
+    ms = median_ms(reps)
     ms_max = ms
     if dist_on:
         t = torch.tensor([ms], device=f"cuda:{dev}", dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms_max = float(t.item())
-    clocks = sampler.summary(t0, t1)
+    clocks = sampler.summary(reps[0]["t0"], reps[-1]["t1"])
     value = world * n * args.steps / (ms_max / 1e3) / 1e9
     ms_per_step = ms_max / args.steps
     bpc = BYTES_PER_CELL[args.storage]
@@ -328,62 +501,57 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "kernel": f"{step_kernel(args.storage)} (fused pull-stream + boundary + BGK collide)",
     }
 
-    # variants and precision (every rank runs them; no collectives inside)
-    variants, precision = {}, {}
+    # storage variants at the same step count (every rank runs them; no collectives inside)
+    variants = {}
     if not args.skip_variants:
-        results = {args.storage: (ms, rho_h, u_h)}
+        results = {args.storage: (reps, healthy)}
         for st in ("f16", "bf16", "f64"):
-            if st == args.storage:
-                continue
-            ms_v, _, _, rho_v, u_v = measure(st, args.steps, args.warmup)
-            results[st] = (ms_v, rho_v, u_v)
-        ref_rho, ref_u = results["f64"][1], results["f64"][2]
-        umax = float(np.max(np.sqrt((ref_u * ref_u).sum(axis=0))))
-        fluid = flags != 1
-        for st, (ms_v, rho_v, u_v) in results.items():
-            glups = n * args.steps / (ms_v / 1e3) / 1e9
+            if st != args.storage:
+                results[st] = measure(st, args.steps, args.warmup, False)
+        for st, (reps_v, healthy_v) in results.items():
+            ms_v = median_ms(reps_v)
             ach = n * BYTES_PER_CELL[st] / (ms_v / args.steps / 1e3) / 1e9
-            variants[st] = {"glups": glups, "ms_per_step": ms_v / args.steps, "hbm_gbs": ach,
-                            "frac": ach / hbm, "bytes_per_cell": BYTES_PER_CELL[st]}
-            if st != "f64":
-                du = np.sqrt(((u_v - ref_u) ** 2).sum(axis=0))[fluid]
-                precision[st] = {
-                    "u_max_err_rel": float(du.max() / umax),
-                    "u_l2_err_rel": float(np.sqrt(np.mean(du**2)) / umax),
-                    "rho_max_err": float(np.max(np.abs(rho_v - ref_rho)[fluid])),
-                    "rho_l2_err": float(np.sqrt(np.mean((rho_v - ref_rho)[fluid] ** 2))),
-                }
-        precision["reference"] = f"f64 GPU build of the same kernel after {args.warmup + args.steps} steps; " \
-                                 f"u errors relative to max|u| = {umax:.4g}"
+            variants[st] = {"glups": n * args.steps / (ms_v / 1e3) / 1e9, "ms_per_step": ms_v / args.steps,
+                            "hbm_gbs": ach, "frac": ach / hbm, "bytes_per_cell": BYTES_PER_CELL[st],
+                            "kernel": step_kernel(st), "healthy": healthy_v, "repeats": public_reps(reps_v)}
         if "f16" in variants and args.storage in variants:
             variants["f16_over_f32_glups"] = variants["f16"]["glups"] / variants[args.storage]["glups"]
 
-    # end to end through the public API with host buffers
+    # errors of the reduced-precision storages after a fixed 5000 steps
+    precision = None
+    if args.precision != "none":
+        precision = precision_leg(torch, args.precision, dev)
+
+    # adjoint cost relative to the forward steps
+    adjoint = None
+    if not args.skip_adjoint:
+        adjoint = adjoint_leg(torch, dev)
+
+    # end to end through the public API with host buffers: upload of the
+    # initial rho / u fields and the flag grid, the equilibrium built on the
+    # device, the steps with per-step FP64 sums to the host, rho / u read back
     e2e = None
     if not args.skip_e2e:
-        import oracle as O
-
-        u0 = np.zeros((3, *SHAPE))
-        u0[0] = INFLOW_U
-        f0_pinned = torch.empty((19, *SHAPE), dtype=torch.float64, pin_memory=True).numpy()
-        f0_pinned[...] = O.feq_field(np.ones(SHAPE), u0)
-        del u0
         from lattice_boltzmann_d3q19_b200 import Lattice
 
+        rho0 = torch.empty(SHAPE, dtype=torch.float64, pin_memory=True).numpy()
+        u0 = torch.empty((3, *SHAPE), dtype=torch.float64, pin_memory=True).numpy()
+        rho0[...] = 1.0
+        u0[...] = 0.0
+        u0[0] = INFLOW_U
         lat = Lattice(SHAPE, TAU, storage=args.storage, inflow_u=(INFLOW_U, 0.0, 0.0), device=dev,
                       cells_per_thread=CELLS_PER_THREAD, staging=STAGING)
-        lat.set_populations(f0_pinned)  # allocate staging outside the timed region
-        # pinned host arrays for the readback, allocated outside the timed region
+        lat.set_equilibrium(rho0, u0)  # allocates the upload staging outside the timed region
         rho_pinned = torch.empty(SHAPE, dtype=torch.float64, pin_memory=True).numpy()
         u_pinned = torch.empty((3, *SHAPE), dtype=torch.float64, pin_memory=True).numpy()
         torch.cuda.synchronize()
         if dist_on:
             torch.distributed.barrier()
         t = time.perf_counter()
-        lat.set_populations(f0_pinned)
         lat.set_flags(flags)
+        lat.set_equilibrium(rho0, u0)
         sums = lat.step_monitor(args.steps)
-        rho_e, u_e = lat.rho_u(out=(rho_pinned, u_pinned))
+        lat.rho_u(out=(rho_pinned, u_pinned))
         torch.cuda.synchronize()
         dt = time.perf_counter() - t
         lat.close()
@@ -391,17 +559,21 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             tt = torch.tensor([dt], device=f"cuda:{dev}", dtype=torch.float64)
             torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
             dt = float(tt.item())
-        out_bytes = 4 * n * 8  # rho and u as f64 (widened on the device for the f32-arithmetic storages)
+        in_bytes = 4 * n * 8 + n  # rho, u (f64) and the flag grid
+        out_bytes = 4 * n * 8     # rho and u as f64
         e2e = {
             "value": world * n * args.steps / dt / 1e9,
             "unit": "GLUPS",
-            "h2d_bytes_per_step": (19 * 8 * n + n) / args.steps,
-            "d2h_bytes_per_step": (5 * 8 * args.steps + out_bytes) / args.steps,
-            "what": "set_populations (pinned f64) + set_flags + step_monitor (per-step FP64 mass/momentum "
-                    "sums to host) + rho_u readback into pinned f64 arrays, wall clock",
+            "h2d_bytes_per_step": in_bytes / args.steps,
+            "d2h_bytes_per_step": (4 * 8 * args.steps + out_bytes) / args.steps,
+            "what": "set_flags + set_equilibrium(rho, u) from pinned f64 host arrays (equilibrium built on the "
+                    "device) + step_monitor (per-step FP64 mass/momentum sums to host) + rho_u readback into "
+                    "pinned f64 arrays, wall clock",
             "mass_drift_rel": float((sums[-1, 0] - sums[0, 0]) / sums[0, 0]),
         }
     sampler.stop()
+    if nvml is not None:
+        nvml.stop()
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
@@ -443,7 +615,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             "l2": f"inputs larger than L2: 2 x {19 * n * {'f64': 8, 'f32': 4}.get(args.storage, 2) / 1e6:.0f} MB "
                   f"population buffers",
             "parallelism": "replicas (one independent lattice per GPU)" if world > 1 else "single GPU",
+            "timing": f"median of {repeats} timed repeats of {args.steps} steps",
         },
+        "repeats": public_reps(reps),
         "roofline": roofline,
         "cpu_baseline": cpu,
         "e2e": e2e,
@@ -452,7 +626,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "healthy": healthy,
         "variants": variants,
         "precision": precision,
-        "adjoint_over_forward": None,
+        "adjoint_over_forward": adjoint,
     }
     print(json.dumps(line), flush=True)
 
@@ -831,6 +1005,10 @@ def main():
     ap.add_argument("--skip-variants", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-adjoint", action="store_true")
+    ap.add_argument("--precision", default="c3", choices=["c3", "c2", "none"],
+                    help="5000-step error leg: 512x256x256 (c3), the headline 256x128x128 (c2) or none")
+    ap.add_argument("--repeats", type=int, default=REPEATS)
     ap.add_argument("--cells-per-thread", type=int, default=0, choices=[0, 1, 2])
     ap.add_argument("--staging", default="auto", choices=["auto", "registers", "tma", "pipelined"])
     ap.add_argument("--workload", default="channel", choices=["channel", "cavity", "sweep", "ensemble", "adjoint", "slab"])

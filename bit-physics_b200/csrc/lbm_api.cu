@@ -4,12 +4,12 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <initializer_list>
 #include <mutex>
+#include <utility>
 #include <string>
 #include <vector>
 
-#include <sys/mman.h>
-#include <unistd.h>
 
 #include "lbm_d3q19.h"
 #include "lbm_handle.h"
@@ -220,21 +220,11 @@ int lbm::api::advance(lbm_lattice* h, void* rho, void* u, double* partials, int*
 namespace {
 
 // Copy a device readback pair (C = double or float) into host f64 arrays.
-// Ask for transparent huge pages on a host output range that is about to be
-// written for the first time (a fresh NumPy array): a 100 MB readback then
-// takes ~50 page faults instead of ~25,000.  A hint only; errors are ignored.
-void hint_huge_pages(void* p, size_t bytes)
-{
-    const uintptr_t page = (uintptr_t)sysconf(_SC_PAGESIZE);
-    const uintptr_t a = ((uintptr_t)p + page - 1) & ~(page - 1), b = ((uintptr_t)p + bytes) & ~(page - 1);
-    if (b > a) (void)madvise((void*)a, b - a, MADV_HUGEPAGE);
-}
-
+// The caller's arrays are used as they are: no paging advice or other change
+// is applied to memory the library does not own.
 int readback_to_host(lbm_lattice* h, const void* drho, const void* du, double* rho, double* u)
 {
     const size_t n = (size_t)h->n;
-    if (rho) hint_huge_pages(rho, sizeof(double) * n);
-    if (u) hint_huge_pages(u, sizeof(double) * 3 * n);
     // f32 values widened to f64 on the device (in the population staging
     // buffer, 19 n doubles) and copied straight into the caller's arrays.
     const bool staged = h->storage != LBM_STORAGE_F64 && (h->staging || ensure_staging(h) == LBM_OK);
@@ -696,8 +686,10 @@ int lbm_step(lbm_lattice* h, int32_t n_steps)
     if ((rc = check_force_ready(h))) return rc;
     int32_t s = 0;
     // Launch-bound small lattices gain from replaying steady-state steps
-    // (two per replay) from a captured CUDA graph.
-    if (n_steps >= 8) {
+    // (two per replay) from a captured CUDA graph.  Any call of three or more
+    // steps captures it (a short warm-up call then leaves the capture and
+    // instantiation behind it, outside a caller's timed loop).
+    if (n_steps >= 3) {
         while (s < n_steps && (h->pre || (h->graph && h->graph_version == h->params_version && h->cur != h->graph_cur))) {
             if ((rc = advance(h, nullptr, nullptr, nullptr))) return rc;
             ++s;
@@ -965,6 +957,26 @@ int ref_params(int nx, int ny, int nz, Params& P)
     return LBM_OK;
 }
 
+// LBM_OK when every non-null pointer is device (or managed) memory of the
+// current GPU; a host pointer or another GPU's memory handed to a kernel
+// would fault the GPU instead of failing here.
+int check_dev_ptrs(std::initializer_list<std::pair<const void*, const char*>> ptrs)
+{
+    int dev = 0;
+    CK(cudaGetDevice(&dev), "cudaGetDevice");
+    for (const auto& pw : ptrs) {
+        if (!pw.first) continue;
+        cudaPointerAttributes attr{};
+        if (cudaPointerGetAttributes(&attr, pw.first) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(LBM_ERR_INVALID, "%s is not a CUDA pointer", pw.second);
+        }
+        const bool ok = attr.type == cudaMemoryTypeManaged || (attr.type == cudaMemoryTypeDevice && attr.device == dev);
+        if (!ok) return fail(LBM_ERR_INVALID, "%s must be device memory of GPU %d", pw.second, dev);
+    }
+    return LBM_OK;
+}
+
 int finish(cudaError_t e, const char* what, cudaStream_t s)
 {
     if (e != cudaSuccess) return cuda_fail(e, what);
@@ -992,6 +1004,7 @@ int lbm_feq_field_dev(const double* rho, const double* u, double* feq, int32_t n
     int rc = ref_params(nx, ny, nz, P);
     if (rc) return rc;
     if (!rho || !u || !feq) return fail(LBM_ERR_INVALID, "null pointer");
+    if ((rc = check_dev_ptrs({{rho, "rho"}, {u, "u"}, {feq, "feq"}}))) return rc;
     return finish(ref_feq_field(P, rho, u, feq, (cudaStream_t)stream), "feq_field", (cudaStream_t)stream);
 }
 
@@ -1001,6 +1014,7 @@ int lbm_density_field_dev(const double* f, double* rho, int32_t nx, int32_t ny, 
     int rc = ref_params(nx, ny, nz, P);
     if (rc) return rc;
     if (!f || !rho) return fail(LBM_ERR_INVALID, "null pointer");
+    if ((rc = check_dev_ptrs({{f, "f"}, {rho, "rho"}}))) return rc;
     return finish(ref_density(P, f, rho, (cudaStream_t)stream), "density_field", (cudaStream_t)stream);
 }
 
@@ -1010,6 +1024,7 @@ int lbm_momentum_field_dev(const double* f, double* mom, int32_t nx, int32_t ny,
     int rc = ref_params(nx, ny, nz, P);
     if (rc) return rc;
     if (!f || !mom) return fail(LBM_ERR_INVALID, "null pointer");
+    if ((rc = check_dev_ptrs({{f, "f"}, {mom, "mom"}}))) return rc;
     return finish(ref_momentum(P, f, mom, (cudaStream_t)stream), "momentum_field", (cudaStream_t)stream);
 }
 
@@ -1020,6 +1035,7 @@ int lbm_macroscopic_velocity_dev(const double* f, const double* force, double* u
     int rc = ref_params(nx, ny, nz, P);
     if (rc) return rc;
     if (!f || !u) return fail(LBM_ERR_INVALID, "null pointer");
+    if ((rc = check_dev_ptrs({{f, "f"}, {force, "force"}, {u, "u"}}))) return rc;
     return finish(ref_macro_velocity(P, f, force, u, (cudaStream_t)stream), "macroscopic_velocity",
                   (cudaStream_t)stream);
 }
@@ -1030,6 +1046,7 @@ int lbm_stream_dev(const double* f_post, double* f_out, int32_t nx, int32_t ny, 
     int rc = ref_params(nx, ny, nz, P);
     if (rc) return rc;
     if (!f_post || !f_out || f_post == f_out) return fail(LBM_ERR_INVALID, "null or aliased pointer");
+    if ((rc = check_dev_ptrs({{f_post, "f_post"}, {f_out, "f_out"}}))) return rc;
     return finish(ref_stream(P, f_post, f_out, (cudaStream_t)stream), "stream", (cudaStream_t)stream);
 }
 
@@ -1040,6 +1057,7 @@ int lbm_bgk_step_dev(const double* f, double* f_out, double tau, const double* f
     int rc = ref_params(nx, ny, nz, P);
     if (rc) return rc;
     if (!f || !f_out || f == f_out) return fail(LBM_ERR_INVALID, "null or aliased pointer");
+    if ((rc = check_dev_ptrs({{f, "f"}, {force, "force"}, {f_out, "f_out"}}))) return rc;
     P.tau = tau;
     return finish(ref_bgk_step(P, f, force, f_out, (cudaStream_t)stream), "bgk_step", (cudaStream_t)stream);
 }
@@ -1051,6 +1069,7 @@ int lbm_bounce_back_y_walls_dev(const double* f, double* f_out, int32_t nx, int3
     int rc = ref_params(nx, ny, nz, P);
     if (rc) return rc;
     if (!f || !f_out || f == f_out) return fail(LBM_ERR_INVALID, "null or aliased pointer");
+    if ((rc = check_dev_ptrs({{f, "f"}, {f_out, "f_out"}}))) return rc;
     for (int a = 0; a < 3; ++a) {
         P.wall_u[FACE_YP][a] = top ? top[a] : 0.0;
         P.wall_u[FACE_YM][a] = bottom ? bottom[a] : 0.0;

@@ -12,18 +12,23 @@
 // scratch in a fixed file-scope device array instead.
 //
 // Limits and sharing:
-//   * the array holds the partial sums of at most LBM_NOALLOC_MAX_CELLS / 256
-//     blocks, so lattices above LBM_NOALLOC_MAX_CELLS cells are rejected;
+//   * the array holds the partial sums of at most LBM_NOALLOC_MAX_CELLS / 128
+//     blocks (5.2 MB per GPU), so lattices above LBM_NOALLOC_MAX_CELLS cells
+//     are rejected;
 //   * it is one array per GPU for the life of the process, shared by every
 //     call on that GPU: two calls whose kernels overlap on the GPU (different
 //     streams, or different host threads) race on it and both results are
 //     undefined -- serialise them;
-//   * the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture begins.
+//   * every call looks up the array's device address (cudaGetSymbolAddress,
+//     not a stream operation) with the caller's device current, so the
+//     address stays right after cudaDeviceReset reloads the module; the first
+//     call on a device loads the module, so make it before any stream capture
+//     begins;
+//   * the blocks are 128 threads, the default block of a lattice handle, so
+//     the sums are bit-identical to lbm_conservation of a default lattice
+//     holding f as its uploaded state.
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 
 #include "lbm_d3q19.h"
 #include "lbm_kernels.cuh"
@@ -32,33 +37,44 @@
 namespace lbm {
 namespace {
 
-constexpr int NOALLOC_BLOCK = 256;
+constexpr int NOALLOC_BLOCK = 128;
 constexpr int NOALLOC_MAX_BLOCKS = (int)(LBM_NOALLOC_MAX_CELLS / NOALLOC_BLOCK);
 
 // Per-block partials (5 doubles each) followed by the 5 final sums.  Every
 // call overwrites all entries it reads, so nothing needs clearing.
 static __device__ __align__(256) double g_noalloc_scratch[(size_t)NOALLOC_MAX_BLOCKS * 5 + 5];
 
-constexpr int MAX_DEVICES = 64;
-std::mutex g_setup_mu;
-double* g_scratch_addr[MAX_DEVICES] = {};
-
-// Device address of the scratch array on the current device (looked up once).
+// Device address of the scratch array on the current device.
 cudaError_t scratch_address(double** out)
+{
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    *out = (double*)p;
+    return cudaSuccess;
+}
+
+// LBM_OK when p is device (or managed) memory of the current device; a host
+// pointer handed to the kernels would fault the GPU instead of failing here.
+int check_dev(const void* p, const char* what)
 {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lk(g_setup_mu);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return e;
-        g_scratch_addr[dev] = (double*)p;
+    if (e != cudaSuccess) return set_error(LBM_ERR_CUDA, cudaGetErrorString(e));
+    cudaPointerAttributes attr{};
+    e = cudaPointerGetAttributes(&attr, p);
+    char msg[160];
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        std::snprintf(msg, sizeof(msg), "lbm_conservation_noalloc: %s is not a CUDA pointer", what);
+        return set_error(LBM_ERR_INVALID, msg);
     }
-    *out = g_scratch_addr[dev];
-    return cudaSuccess;
+    const bool ok = attr.type == cudaMemoryTypeManaged || (attr.type == cudaMemoryTypeDevice && attr.device == dev);
+    if (!ok) {
+        std::snprintf(msg, sizeof(msg), "lbm_conservation_noalloc: %s must be device memory of GPU %d", what, dev);
+        return set_error(LBM_ERR_INVALID, msg);
+    }
+    return LBM_OK;
 }
 
 // The 5 final sums -> the caller's 4 outputs {sum rho, sum m_x, sum m_y, sum m_z}.
@@ -86,6 +102,10 @@ extern "C" int lbm_conservation_noalloc(const double* f, const uint8_t* flags, i
                       n, (long long)LBM_NOALLOC_MAX_CELLS);
         return set_error(LBM_ERR_INVALID, msg);
     }
+    int rc = check_dev(f, "f");
+    if (rc == LBM_OK) rc = check_dev(out4, "out4");
+    if (rc == LBM_OK && flags) rc = check_dev(flags, "flags");
+    if (rc != LBM_OK) return rc;
     double* scratch = nullptr;
     cudaError_t e = scratch_address(&scratch);
     if (e != cudaSuccess) return set_error(LBM_ERR_CUDA, cudaGetErrorString(e));

@@ -14,9 +14,14 @@
 // vector stores to global memory.  Cells that need a boundary rule use
 // k_step's resolve_state (global reloads).
 //
-// Every mbarrier wait is bounded; a wait that runs out sets *P.err (the host
-// reports it and the state is invalid) and the kernel runs to its normal end,
-// consuming every stage it issued.  No multicast.
+// Every mbarrier wait is bounded by a deadline on the global nanosecond
+// timer.  A wait that runs out sets *P.err (the host reports it and the state
+// is invalid) and a block-wide abort flag in shared memory: from then on the
+// producer issues no copy and no thread of the block waits again, so the
+// error path ends quickly.  Before the producer warp exits it waits (bounded
+// again) for the last copy group it issued into every stage, so no block
+// retires with bulk copies still writing into its shared memory.  No
+// multicast.
 #pragma once
 
 #include "lbm_kernels.cuh"
@@ -27,7 +32,7 @@ constexpr int TMA_CONSUMER_WARPS = 8;
 constexpr int TMA_CONSUMERS = 32 * TMA_CONSUMER_WARPS;  // cell threads
 constexpr int TMA_THREADS = TMA_CONSUMERS + 32;         // + one producer warp
 constexpr int TMA_MAX_STAGES = 4;
-constexpr unsigned TMA_WAIT_LIMIT = 1u << 22;  // try_wait polls before giving up
+constexpr unsigned long long TMA_WAIT_NS = 500000000ull;  // 0.5 s per wait before giving up
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
 {
@@ -45,18 +50,27 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
                  ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
-// Bounded wait for the phase with the given parity; true when it completed.
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Wait for the phase with the given parity, for at most TMA_WAIT_NS of
+// wall time; true when it completed.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
 {
     const uint32_t a = smem_u32(bar);
-    for (unsigned it = 0; it < TMA_WAIT_LIMIT; ++it) {
+    const unsigned long long t0 = global_ns();
+    for (;;) {
         uint32_t done;
         asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
                      "selp.u32 %0, 1, 0, p;\n\t}"
                      : "=r"(done) : "r"(a), "r"(parity) : "memory");
         if (done) return true;
+        if (global_ns() - t0 > TMA_WAIT_NS) return false;
     }
-    return false;
 }
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar)
@@ -121,6 +135,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(Params P, Streams<t
     extern __shared__ __align__(128) unsigned char tma_smem[];
     __shared__ __align__(8) uint64_t full[TMA_MAX_STAGES];
     __shared__ __align__(8) uint64_t empty[TMA_MAX_STAGES];
+    __shared__ int abort_flag;  // set by the first wait of the block that runs out
     // Ring base rounded up to 128 bytes (the launch allocates the slack): every
     // bulk-copy destination is then a multiple of the 16-byte row size.
     T* ring = reinterpret_cast<T*>((reinterpret_cast<uintptr_t>(tma_smem) + 127) & ~(uintptr_t)127);
@@ -132,18 +147,37 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(Params P, Streams<t
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], TMA_CONSUMER_WARPS);
         }
+        abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    volatile int* abort_v = &abort_flag;
+    auto give_up = [&]() {
+        *abort_v = 1;
+        atomicExch(P.err, 1);
+    };
     double cons[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     if (warp == TMA_CONSUMER_WARPS) {
         // producer: refill each stage once its previous tile has been consumed
         int k = 0;
         for (int t = blockIdx.x; t < G.ntiles; t += gridDim.x, ++k) {
             const int s = k % G.stages;
-            if (k >= G.stages && !mbar_wait(&empty[s], (uint32_t)(k / G.stages - 1) & 1u) && lane == 0)
-                atomicExch(P.err, 1);
+            if (__any_sync(0xffffffffu, *abort_v != 0)) break;
+            bool ok = true;
+            if (k >= G.stages) ok = mbar_wait(&empty[s], (uint32_t)(k / G.stages - 1) & 1u);
+            if (!__all_sync(0xffffffffu, ok)) {
+                if (lane == 0) give_up();
+                break;
+            }
             tma_issue_tile<T>(P, S, G, t, ring + (size_t)s * G.stage_elems, &full[s], lane);
+        }
+        // Drain: the last copy group issued into each stage (tile k - 1 - j
+        // sits in stage (k - 1 - j) % stages) must land before the block may
+        // retire, whatever happened to the consumers.
+        for (int j = 0; j < G.stages && j < k; ++j) {
+            const int kk = k - 1 - j;
+            const bool ok = mbar_wait(&full[kk % G.stages], (uint32_t)(kk / G.stages) & 1u);
+            if (!ok && lane == 0) give_up();
         }
     } else {
         int k = 0;
@@ -158,9 +192,15 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(Params P, Streams<t
             unsigned short both_next = 0;
             if (P.has_flags && tid < tile_pairs)
                 both_next = __ldg(reinterpret_cast<const unsigned short*>(P.flags + tile_base + 2 * tid));
-            // A wait that runs out raises the error word and the thread carries
-            // on (the host discards the state); every loop stays bounded.
-            if (!mbar_wait(&full[s], (uint32_t)(k / G.stages) & 1u)) atomicExch(P.err, 1);
+            // After a wait of this block ran out, no thread waits again (the
+            // host discards the state); the producer drains its copies.
+            // Warp-uniform decisions: a consumer warp leaves the loop as a whole.
+            if (__any_sync(0xffffffffu, *abort_v != 0)) break;
+            const bool ok = mbar_wait(&full[s], (uint32_t)(k / G.stages) & 1u);
+            if (!__all_sync(0xffffffffu, ok)) {
+                if (lane == 0) give_up();
+                break;
+            }
             const T* st = ring + (size_t)s * G.stage_elems;
             for (int p = tid; p < tile_pairs; p += TMA_CONSUMERS) {
                 const int c0 = 2 * p;

@@ -171,3 +171,31 @@ def f64(a) -> np.ndarray:
 
 def ptr(a: np.ndarray | None, ctype=_dp):
     return None if a is None else a.ctypes.data_as(ctype)
+
+
+_MADV_HUGEPAGE = 14
+_libc = None
+
+
+def fresh_host_array(shape) -> np.ndarray:
+    """np.empty(shape) float64 with transparent huge pages requested for it
+    (Linux madvise): a readback of ~100 MB into a fresh array then takes
+    ~50 page faults instead of ~25,000.  Only for arrays allocated here;
+    caller-owned output arrays are never advised.  A hint: failures are
+    ignored."""
+    global _libc
+    a = np.empty(shape)
+    try:
+        if _libc is None:
+            _libc = C.CDLL(None, use_errno=True)
+            _libc.madvise.argtypes = [C.c_void_p, C.c_size_t, C.c_int]
+            _libc.madvise.restype = C.c_int
+        page = 4096
+        lo = (a.ctypes.data + page - 1) & ~(page - 1)
+        hi = (a.ctypes.data + a.nbytes) & ~(page - 1)
+        if hi > lo:
+            _libc.madvise(C.c_void_p(lo), C.c_size_t(hi - lo), _MADV_HUGEPAGE)
+    except (OSError, AttributeError):
+        pass
+    return a
+

@@ -201,8 +201,8 @@ class Lattice:
         float64 of those shapes), e.g. views of pinned memory, which the
         device-to-host copy then fills at full speed."""
         if out is None:
-            rho = np.empty(self.shape)
-            u = np.empty((3, *self.shape))
+            rho = N.fresh_host_array(self.shape)
+            u = N.fresh_host_array((3, *self.shape))
         else:
             rho, u = out
             for a, shape, name in ((rho, self.shape, "rho"), (u, (3, *self.shape), "u")):
@@ -218,8 +218,8 @@ class Lattice:
         steps = list(range(0, n_steps + 1, every))
         if steps[-1] != n_steps:
             steps.append(n_steps)
-        rho = np.empty((len(steps), *self.shape))
-        u = np.empty((len(steps), 3, *self.shape))
+        rho = N.fresh_host_array((len(steps), *self.shape))
+        u = N.fresh_host_array((len(steps), 3, *self.shape))
         N.check(N.lib().lbm_run_capture(self._h, int(n_steps), int(every), N.ptr(rho), N.ptr(u)))
         return np.array(steps), rho, u
 

@@ -281,13 +281,17 @@ int lbm_tape_destroy(lbm_tape* t);
  * sum m_z} of a population array f (19, nx, ny, nz, f64, device memory) over
  * its non-solid cells (flags: optional device uint8 cell types), written to
  * out4 (4 doubles, device memory), enqueued on `stream` (NULL: the legacy
- * default stream).  The same reduction as lbm_conservation on a lattice
- * holding f, but it allocates nothing: its scratch is one fixed device array
- * per GPU, for callers that cannot call cudaMalloc where they need the sums
- * (another allocator owns the device memory, or a step loop must not be
- * stalled by an allocation).  At most LBM_NOALLOC_MAX_CELLS cells; calls that
- * overlap on one GPU race on the shared array.  The first call on a device
- * looks up the array's address and should come before any stream capture. */
+ * default stream).  f, flags and out4 must be device memory of the current
+ * GPU (LBM_ERR_INVALID otherwise).  The result is bit-identical to
+ * lbm_conservation of an f64 lattice with the default block size holding f
+ * as its uploaded state (same 128-cell blocks, same reduction order), and
+ * equal up to FP64 rounding for other block sizes.  It allocates nothing: its
+ * scratch is one fixed device array per GPU, for callers that cannot call
+ * cudaMalloc where they need the sums (another allocator owns the device
+ * memory, or a step loop must not be stalled by an allocation).  At most
+ * LBM_NOALLOC_MAX_CELLS cells; calls that overlap on one GPU race on the
+ * shared array.  The first call on a device loads the module that holds the
+ * array and should come before any stream capture. */
 #define LBM_NOALLOC_MAX_CELLS 16777216LL
 int lbm_conservation_noalloc(const double* f, const uint8_t* flags, int32_t nx, int32_t ny, int32_t nz,
                              double* out4, void* stream);

@@ -1,7 +1,8 @@
 """Regenerate the golden fixtures in this directory from the reference itself.
 
-Runs only where the Bit-Physics reference tree is mounted (default
-``/root/reference``; override with ``BITPHYSICS_REF``).  It imports the
+Runs only where the Bit-Physics reference tree is mounted; its root is
+given by the ``BITPHYSICS_REF`` environment variable (required, e.g.
+``BITPHYSICS_REF=/path/to/Bit-Physics python make_golden.py``).  It imports the
 Phase-1 NumPy reference package ``packages/lattice-boltzmann-d3q19``
 read-only -- the frozen parent that the Stack-E Warp port reproduces
 byte-for-byte (docs/sim-specs/lattice/lattice-boltzmann-d3q19/
@@ -42,7 +43,9 @@ from pathlib import Path
 import numpy as np
 
 OUT = Path(__file__).resolve().parent
-REF = Path(os.environ.get("BITPHYSICS_REF", "/root/reference"))
+if not os.environ.get("BITPHYSICS_REF"):
+    sys.exit("make_golden.py: set BITPHYSICS_REF to the root of the Bit-Physics reference tree")
+REF = Path(os.environ["BITPHYSICS_REF"])
 
 
 def _import_reference():

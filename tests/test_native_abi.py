@@ -95,3 +95,40 @@ def test_no_device_is_reported_not_faked():
 
     with pytest.raises(N.LbmError):
         R.stream(f)
+
+
+def _dev_calls_with(ptrs, shape=(3, 2, 2)):
+    """Every stateless device-pointer entry point called with the given
+    pointers (ptrs[k] for its k-th array argument)."""
+    lib = N.lib()
+    p = [C.c_void_p(a.ctypes.data) for a in ptrs]
+    nx, ny, nz = shape
+    return {
+        "feq_field": lib.lbm_feq_field_dev(p[0], p[1], p[2], nx, ny, nz, None),
+        "density_field": lib.lbm_density_field_dev(p[0], p[1], nx, ny, nz, None),
+        "momentum_field": lib.lbm_momentum_field_dev(p[0], p[1], nx, ny, nz, None),
+        "macroscopic_velocity": lib.lbm_macroscopic_velocity_dev(p[0], None, p[1], nx, ny, nz, None),
+        "stream": lib.lbm_stream_dev(p[0], p[1], nx, ny, nz, None),
+        "bgk_step": lib.lbm_bgk_step_dev(p[0], p[1], 0.7, None, nx, ny, nz, None),
+        "bounce_back": lib.lbm_bounce_back_y_walls_dev(p[0], p[1], nx, ny, nz, None, None, None),
+        "conservation_noalloc": lib.lbm_conservation_noalloc(p[0], None, nx, ny, nz, p[1], None),
+    }
+
+
+def test_dev_entry_points_refuse_host_pointers_without_a_device():
+    """Host NumPy pointers handed to the device-pointer entry points come
+    back as an error status (no device here: before any kernel could run)."""
+    if N.device_count() > 0:
+        pytest.skip("a CUDA device is present (the gpu-marked test covers it)")
+    arrs = [np.zeros(19 * 12) for _ in range(3)]
+    for name, rc in _dev_calls_with(arrs).items():
+        assert rc < 0, name
+
+
+@pytest.mark.gpu
+def test_dev_entry_points_reject_host_pointers():
+    """On a GPU, host memory passed where device memory is required is
+    rejected with LBM_ERR_INVALID before any launch (a kernel would fault)."""
+    arrs = [np.zeros(19 * 12) for _ in range(3)]
+    for name, rc in _dev_calls_with(arrs).items():
+        assert rc == N.LBM_ERR_INVALID, (name, rc, N.lib().lbm_last_error())

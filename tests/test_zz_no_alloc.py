@@ -54,7 +54,18 @@ def test_noalloc_matches_lattice_conservation_on_consecutive_calls(with_flags):
             assert _noalloc(f_dev, flags_dev, shape, out) == N.LBM_OK, N.lib().lbm_last_error()
             torch.cuda.synchronize()
             got = out.cpu().numpy()
-            assert np.allclose(got, expected, rtol=1e-13, atol=1e-13), (got, expected)
+            # same 128-cell blocks and reduction order as a default lattice
+            assert got.tobytes() == np.asarray(expected, np.float64).tobytes(), (got, expected)
+
+
+def test_noalloc_rejects_host_pointers():
+    shape = (6, 5, 4)
+    f_host = random_state(shape, 3)
+    out = torch.empty(4, dtype=torch.float64, device="cuda")
+    rc = N.lib().lbm_conservation_noalloc(C.c_void_p(f_host.ctypes.data), None, *shape,
+                                          C.c_void_p(out.data_ptr()), None)
+    assert rc == N.LBM_ERR_INVALID
+    assert b"device memory" in N.lib().lbm_last_error() or b"CUDA pointer" in N.lib().lbm_last_error()
 
 
 def test_noalloc_rejects_lattices_beyond_its_fixed_scratch():
