@@ -216,8 +216,8 @@ def step_kernel(storage: str) -> str:
         return f"k_step_tma<{storage}>"
     if STAGING == "pipelined" and storage in ("f16", "bf16") and CELLS_PER_THREAD in (0, 2):
         return f"k_step2_pipe<{storage}>"
-    cpt = CELLS_PER_THREAD or (1 if storage == "f64" else 2)
-    return f"{'k_step2' if cpt == 2 else 'k_step'}<{storage}>"
+    cpt = CELLS_PER_THREAD or (1 if storage == "f64" else (4 if storage in ("f16", "bf16") else 2))
+    return f"{ {1: 'k_step', 2: 'k_step2', 4: 'k_step4'}[cpt] }<{storage}>"
 
 
 def make_lattice(storage: str, flags, device: int):
@@ -663,8 +663,8 @@ def run_cavity(args):
     out, out_proxy = {}, {}
     n = int(np.prod(shape))
 
-    def timed(storage, kwargs):
-        lat = Lattice(shape, tau, storage=storage, **kwargs)
+    def timed(storage, kwargs, staging="auto"):
+        lat = Lattice(shape, tau, storage=storage, staging=staging, **kwargs)
         lat.set_stream(stream.cuda_stream)
         lat.set_equilibrium()
         lat.step(args.warmup)
@@ -676,7 +676,9 @@ def run_cavity(args):
 
     for storage in ("f32", "f16", "f64"):
         out[storage] = timed(storage, kw)
+        out[storage + "_persistent"] = timed(storage, kw, "persistent")
         out_proxy[storage] = timed(storage, proxy)
+        out_proxy[storage + "_persistent"] = timed(storage, proxy, "persistent")
     cpu = O.OracleLattice(shape, tau, periodic=0, wall_velocity=Lattice._wall_array(kw["wall_velocity"]))
     cpu.set_populations(O.feq_field(np.ones(shape), np.zeros((3, *shape))))
     cpu_steps = min(steps, int(os.environ.get("LBM_CAVITY_CPU_STEPS", "200")))
@@ -1009,8 +1011,8 @@ def main():
     ap.add_argument("--precision", default="c3", choices=["c3", "c2", "none"],
                     help="5000-step error leg: 512x256x256 (c3), the headline 256x128x128 (c2) or none")
     ap.add_argument("--repeats", type=int, default=REPEATS)
-    ap.add_argument("--cells-per-thread", type=int, default=0, choices=[0, 1, 2])
-    ap.add_argument("--staging", default="auto", choices=["auto", "registers", "tma", "pipelined"])
+    ap.add_argument("--cells-per-thread", type=int, default=0, choices=[0, 1, 2, 4])
+    ap.add_argument("--staging", default="auto", choices=["auto", "registers", "tma", "pipelined", "persistent"])
     ap.add_argument("--workload", default="channel", choices=["channel", "cavity", "sweep", "ensemble", "adjoint", "slab"])
     args = ap.parse_args()
     global CELLS_PER_THREAD, STAGING

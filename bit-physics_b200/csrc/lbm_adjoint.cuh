@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(256) k_adjoint_plain(Params P, Streams<typenam
     CellMoments<C> mo{C(0), C(0), C(0), C(0)};
 #pragma unroll
     for (int d = 0; d < Q; ++d) {
-        const C v = M::load(S.src[d] + nb.src(d), d);
+        const C v = M::load(P, S.src[d] + nb.src(d), d);
         mo.rho += v;
         if (cx(d)) mo.mx += C(cx(d)) * v;
         if (cy(d)) mo.my += C(cy(d)) * v;
@@ -367,7 +367,7 @@ __global__ void __launch_bounds__(128) k_adjoint_special(Params P, Streams<typen
     const int type = fl & 3;
     const Nbr nb = make_nbr(P, x, y, z);
     C f[Q], lam[Q];
-    gather<M>(S, nb, f);
+    gather<M>(P, S, nb, f);
     resolve_state<M>(P, S, idx, x, y, z, fl, nb, f);
     const double da = cell_lambda<M, FM, LEVEL>(P, io, idx, x, y, z, adj_moments<M>(f), lam);
     if (FM == FORCE_DRAG && io.dalpha) io.dalpha[idx] += da;
@@ -385,7 +385,7 @@ __global__ void __launch_bounds__(128) k_adjoint_special(Params P, Streams<typen
     const uint32_t bb = (fl & FLAG_NEAR_SOLID) ? P.bbmask[idx] & CW_MASK_BITS : 0u;
     if (type == CELL_OUTFLOW) {
         // own state came from x - 1; the x + 1 outflow cell copies B_x(g(x))
-        gather<M>(S, nb, f);
+        gather<M>(P, S, nb, f);
         if (face || bb) boundary_fix<M>(P, S, nb, x, y, z, idx, face, bb, f);
 #pragma unroll
         for (int d = 0; d < Q; ++d) lam[d] = C(0);
@@ -416,7 +416,7 @@ __global__ void __launch_bounds__(256) k_adjoint_final(Params P, Streams<typenam
     }
     C f[Q], lam[Q];
 #pragma unroll
-    for (int d = 0; d < Q; ++d) f[d] = M::load(S.src[d] + idx, d);
+    for (int d = 0; d < Q; ++d) f[d] = M::load(P, S.src[d] + idx, d);
     const double da = cell_lambda<M, FM, ADJ_FINAL>(P, io, idx, x, y, z, adj_moments<M>(f), lam);
     if (FM == FORCE_DRAG && io.dalpha) io.dalpha[idx] += da;
     if (io.grad_f0) {

@@ -147,6 +147,15 @@ void rebuild_params(lbm_lattice* h)
     }
     P.omega = (float)(1.0 / d.tau);
     P.pref = (float)(1.0 - 0.5 / d.tau);
+    // 16-bit storage reference: feq(1, storage_ref_u) - w, reciprocal form.
+    const bool storage16 = h->storage == LBM_STORAGE_F16_SHIFT || h->storage == LBM_STORAGE_BF16_SHIFT;
+    const double rx = d.storage_ref_u[0], ry = d.storage_ref_u[1], rz = d.storage_ref_u[2];
+    const double r_sq = rx * rx + ry * ry + rz * rz;
+    for (int q = 0; q < Q; ++q) {
+        double cu = (double)cx(q) * rx + (double)cy(q) * ry + (double)cz(q) * rz;
+        const double feq = P.w[q] * 1.0 * (1.0 + cu * P.inv_cs2 + cu * cu * P.inv_two_cs4 - r_sq * P.inv_two_cs2);
+        P.shift_h[q] = storage16 ? (float)(feq - P.w[q]) : 0.0f;
+    }
 }
 
 }  // namespace
@@ -175,6 +184,11 @@ cudaError_t lbm::api::launch(lbm_lattice* h, int kernel, const void* src, void* 
     a.tma_grid = 0;
     a.pipe_grid = kernel == KERNEL_STEP ? h->pipe_grid : 0;
     a.sums_grid = kernel == KERNEL_STEP ? h->sums_grid : 0;
+    a.rule_quads = h->rule_quads;
+    a.rule_count = h->rule_count;
+    a.side = h->side;
+    a.fork = h->ev_fork;
+    a.join = h->ev_join;
     if (kernel == KERNEL_STEP && h->use_tma) {
         a.tma_grid = h->tma_grid;
         a.tile = h->tile;
@@ -185,6 +199,19 @@ cudaError_t lbm::api::launch(lbm_lattice* h, int kernel, const void* src, void* 
 }
 
 namespace {
+
+// The quads k_step4 leaves to k_step4_rules, from the current flags and
+// walled faces (four-cell lattices only).
+int refresh_rule_quads(lbm_lattice* h)
+{
+    if (h->vec != 4) return LBM_OK;
+    int* count = h->rule_quads + h->n / 4;
+    CK(launch_list_rule_quads(h->P, h->rule_quads, count, h->stream), "rule quad list");
+    CK(cudaMemcpyAsync(&h->rule_count, count, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "rule quad count");
+    CK(cudaStreamSynchronize(h->stream), "rule quad sync");
+    h->params_version += 1;  // a captured step graph holds the old count
+    return LBM_OK;
+}
 
 int ensure_staging(lbm_lattice* h)
 {
@@ -321,14 +348,22 @@ int lbm_create(const lbm_desc* desc, lbm_lattice** out)
         return fail(LBM_ERR_INVALID, "unknown force mode %d", desc->force_mode);
     if (!(desc->tau > 0.5)) return fail(LBM_ERR_INVALID, "tau must be > 0.5 (got %g)", desc->tau);
     if (desc->periodic < 0 || desc->periodic > 7) return fail(LBM_ERR_INVALID, "periodic mask must be 0..7");
+    for (int a = 0; a < 3; ++a)
+        if (!(desc->storage_ref_u[a] > -0.5 && desc->storage_ref_u[a] < 0.5))
+            return fail(LBM_ERR_INVALID, "storage_ref_u components must lie in (-0.5, 0.5)");
     if (desc->block_size != 0 && (desc->block_size % 32 != 0 || desc->block_size < 32 || desc->block_size > 256))
         return fail(LBM_ERR_INVALID, "block_size must be 0 or a multiple of 32 in [32, 256]");
-    if (desc->cells_per_thread < 0 || desc->cells_per_thread > 2)
-        return fail(LBM_ERR_INVALID, "cells_per_thread must be 0 (auto), 1 or 2");
-    if (desc->staging < LBM_STAGING_AUTO || desc->staging > LBM_STAGING_PIPELINED)
-        return fail(LBM_ERR_INVALID, "staging must be LBM_STAGING_AUTO, _REGISTERS, _TMA or _PIPELINED");
+    if (desc->cells_per_thread < 0 || desc->cells_per_thread > 4 || desc->cells_per_thread == 3)
+        return fail(LBM_ERR_INVALID, "cells_per_thread must be 0 (auto), 1, 2 or 4");
+    if (desc->staging < LBM_STAGING_AUTO || desc->staging > LBM_STAGING_PERSISTENT)
+        return fail(LBM_ERR_INVALID, "staging must be LBM_STAGING_AUTO, _REGISTERS, _TMA, _PIPELINED or _PERSISTENT");
     if (desc->cells_per_thread == 2 && (desc->storage == LBM_STORAGE_F64 || desc->nz % 2 != 0))
         return fail(LBM_ERR_UNSUPPORTED, "cells_per_thread = 2 needs f32/f16/bf16 storage and an even nz");
+    const bool storage16 = desc->storage == LBM_STORAGE_F16_SHIFT || desc->storage == LBM_STORAGE_BF16_SHIFT;
+    if (desc->cells_per_thread == 4 && (!storage16 || desc->nz % 4 != 0))
+        return fail(LBM_ERR_UNSUPPORTED, "cells_per_thread = 4 needs f16/bf16 storage and nz a multiple of 4");
+    if (desc->cells_per_thread == 4 && desc->staging != LBM_STAGING_AUTO && desc->staging != LBM_STAGING_REGISTERS)
+        return fail(LBM_ERR_UNSUPPORTED, "cells_per_thread = 4 runs with register staging only");
     int ndev = lbm_device_count();
     if (ndev == 0) return fail(LBM_ERR_NO_DEVICE, "no CUDA device available");
     if (desc->device < 0 || desc->device >= ndev) return fail(LBM_ERR_INVALID, "device %d out of range", desc->device);
@@ -345,9 +380,13 @@ int lbm_create(const lbm_desc* desc, lbm_lattice** out)
     h->block = desc->block_size ? desc->block_size : 128;
     // Two cells per thread (packed f32x2 arithmetic) cuts the instructions
     // per cell; measured on the 256x128x128 sphere channel: f16 41 -> 50
-    // GLUPS, f32 unchanged (bandwidth-bound).  Needs an even nz.
+    // GLUPS, f32 unchanged (bandwidth-bound).  Needs an even nz.  The 16-bit
+    // storages take four (k_step4) when nz is a multiple of 4 and the staging
+    // is the default: 78.6 against 66.0 GLUPS (f16, 256x128x128 without flags).
     if (desc->cells_per_thread)
         h->vec = desc->cells_per_thread;
+    else if (storage16 && desc->nz % 4 == 0 && (desc->staging == LBM_STAGING_AUTO || desc->staging == LBM_STAGING_REGISTERS))
+        h->vec = 4;
     else
         h->vec = desc->storage != LBM_STORAGE_F64 && desc->nz % 2 == 0 ? 2 : 1;
     auto cleanup = [&](int code) {
@@ -393,7 +432,7 @@ int lbm_create(const lbm_desc* desc, lbm_lattice** out)
     }
     // Steps with FP64 sums (two cells per thread) run one block per resident
     // slot, each thread looping over pairs: one partial row per block.
-    if (h->storage != LBM_STORAGE_F64 && h->vec == 2) {
+    if (h->storage != LBM_STORAGE_F64 && h->vec >= 2) {
         h->sums_grid = sums_grid_fast(h->storage, desc->force_mode, h->block);
         if (h->sums_grid <= 0) return cleanup(fail(LBM_ERR_CUDA, "step with sums: no resident blocks"));
     }
@@ -411,7 +450,25 @@ int lbm_create(const lbm_desc* desc, lbm_lattice** out)
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->err, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(h->err, 0, sizeof(int));
     if (e != cudaSuccess) return cleanup(cuda_fail(e, "reduction scratch allocation"));
+    if (desc->staging == LBM_STAGING_PERSISTENT) {
+        int coop = 0;
+        if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, desc->device) != cudaSuccess || !coop) {
+            cudaGetLastError();
+            return cleanup(fail(LBM_ERR_UNSUPPORTED, "persistent staging needs cooperative launch support"));
+        }
+        e = cudaMalloc((void**)&h->bar, sizeof(GridBarrier));
+        if (e != cudaSuccess) return cleanup(cuda_fail(e, "grid barrier allocation"));
+        h->persist = true;
+    }
+    if (h->vec == 4) {
+        e = cudaMalloc((void**)&h->rule_quads, sizeof(int) * ((size_t)h->n / 4 + 1));
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming);
+        if (e != cudaSuccess) return cleanup(cuda_fail(e, "four-cell step set-up"));
+    }
     rebuild_params(h);
+    if (int rc2 = refresh_rule_quads(h)) return cleanup(rc2);
     // Rest state f = w_i (rho = 1, u = 0).
     e = launch_feq_init(h->storage, h->P, nullptr, nullptr, h->buf[0], h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -428,10 +485,14 @@ int lbm_destroy(lbm_lattice* h)
     cudaSetDevice(h->desc.device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->graph) cudaGraphExecDestroy(h->graph);
+    if (h->side) cudaStreamSynchronize(h->side);
     void* ptrs[] = {h->buf[0], h->buf[1], h->flags, h->bbmask, h->force, h->poro, h->rho,
-                    h->u, h->partials, h->sums, h->staging, h->monitor, h->err};
+                    h->u, h->partials, h->sums, h->staging, h->monitor, h->err, h->diag, h->rule_quads, h->bar};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
+    if (h->side) cudaStreamDestroy(h->side);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return LBM_OK;
@@ -461,7 +522,8 @@ static int check_device_error(lbm_lattice* h)
     CK(cudaStreamSynchronize(h->stream), "stream sync");
     if (flag) {
         cudaMemsetAsync(h->err, 0, sizeof(int), h->stream);
-        return fail(LBM_ERR_CUDA, "a step kernel's shared-memory pipeline wait timed out; the state is invalid");
+        return fail(LBM_ERR_CUDA, "a step kernel's bounded wait (shared-memory pipeline or grid barrier) timed out; "
+                                  "the state is invalid");
     }
     return LBM_OK;
 }
@@ -541,7 +603,7 @@ int lbm_set_flags(lbm_lattice* h, const uint8_t* flags)
     if (!flags) {
         h->has_flags = false;
         rebuild_params(h);
-        return LBM_OK;
+        return refresh_rule_quads(h);
     }
     const size_t n = (size_t)h->n;
     for (size_t i = 0; i < n; ++i)
@@ -565,7 +627,7 @@ int lbm_set_flags(lbm_lattice* h, const uint8_t* flags)
         h->pre = true;
     }
     CK(cudaStreamSynchronize(h->stream), "flag sync");
-    return LBM_OK;
+    return refresh_rule_quads(h);
 }
 
 int lbm_set_force_field(lbm_lattice* h, const double* force)
@@ -685,6 +747,28 @@ int lbm_step(lbm_lattice* h, int32_t n_steps)
     if (n_steps < 0) return fail(LBM_ERR_INVALID, "negative step count");
     if ((rc = check_force_ready(h))) return rc;
     int32_t s = 0;
+    if (h->persist && n_steps >= 2) {
+        if (h->pre) {
+            if ((rc = advance(h, nullptr, nullptr, nullptr))) return rc;
+            ++s;
+        }
+        const int32_t k = n_steps - s;
+        if (k > 0) {
+            LaunchArgs a;
+            a.P = h->P;
+            a.src = h->buf[h->cur];
+            a.dst = h->buf[h->cur ^ 1];
+            a.block = 256;
+            a.vec = h->vec;
+            a.stream = h->stream;
+            CK(launch_persistent(h->storage, h->desc.force_mode, a, k, h->bar, h->persist_missing,
+                                 h->persist_timeout_ns, nullptr),
+               "persistent step launch");
+            h->cur ^= (k & 1);
+            h->steps += k;
+        }
+        return LBM_OK;
+    }
     // Launch-bound small lattices gain from replaying steady-state steps
     // (two per replay) from a captured CUDA graph.  Any call of three or more
     // steps captures it (a short warm-up call then leaves the capture and
@@ -709,6 +793,17 @@ int lbm_step(lbm_lattice* h, int32_t n_steps)
 }
 
 int64_t lbm_step_count(const lbm_lattice* h) { return h ? h->steps : -1; }
+
+int lbm_test_barrier_limit(lbm_lattice* h, int32_t missing_arrivals, int64_t timeout_ns)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!h->persist) return fail(LBM_ERR_STATE, "the lattice was not created with LBM_STAGING_PERSISTENT");
+    if (missing_arrivals < 0) return fail(LBM_ERR_INVALID, "missing_arrivals must be >= 0");
+    h->persist_missing = (unsigned)missing_arrivals;
+    h->persist_timeout_ns = timeout_ns > 0 ? (unsigned long long)timeout_ns : 2000000000ull;
+    return LBM_OK;
+}
 
 int lbm_get_rho_u(lbm_lattice* h, double* rho, double* u)
 {
@@ -901,6 +996,33 @@ int lbm_plane_get(lbm_lattice* h, int32_t x, uint32_t dir_mask, void* dst) { ret
 int lbm_plane_put(lbm_lattice* h, int32_t x, uint32_t dir_mask, const void* src)
 {
     return plane_copy(h, x, dir_mask, const_cast<void*>(src), false);
+}
+
+int lbm_diagnostics(lbm_lattice* h, double dx_phys, double* out6)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!out6) return fail(LBM_ERR_INVALID, "null output");
+    if (!(dx_phys > 0.0)) return fail(LBM_ERR_INVALID, "dx_phys must be > 0");
+    if ((rc = check_force_ready(h))) return rc;
+    if (!h->diag) CK(cudaMalloc((void**)&h->diag, sizeof(double) * (DIAG_SCRATCH + 6)), "diagnostics scratch");
+    if ((rc = observe_rho_u(h, h->rho, h->u))) return rc;
+    const double* rho = (const double*)h->rho;
+    const double* u = (const double*)h->u;
+    if (h->storage != LBM_STORAGE_F64) {
+        // the f32 readback widened to f64, as lbm_get_rho_u hands it out
+        if ((rc = ensure_staging(h))) return rc;
+        const size_t n = (size_t)h->n;
+        CK(launch_widen((const float*)h->rho, h->staging, n, h->stream), "rho widen");
+        CK(launch_widen((const float*)h->u, h->staging + n, 3 * n, h->stream), "u widen");
+        rho = h->staging;
+        u = h->staging + n;
+    }
+    CK(launch_diagnostics(h->P, rho, u, dx_phys, h->diag, h->diag + DIAG_SCRATCH, h->stream), "diagnostics");
+    CK(cudaMemcpyAsync(out6, h->diag + DIAG_SCRATCH, sizeof(double) * 6, cudaMemcpyDeviceToHost, h->stream),
+       "diagnostics copy");
+    CK(cudaStreamSynchronize(h->stream), "diagnostics sync");
+    return LBM_OK;
 }
 
 int lbm_check_health(lbm_lattice* h)

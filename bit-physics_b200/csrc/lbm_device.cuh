@@ -106,6 +106,10 @@ struct Params {
     float body_force_f[3];
     float drag_kf;
     float inflow_h[Q];  // feq(inflow) - w
+    // 16-bit storages: the stored value of direction d is the deviation of f
+    // from feq_d(1, storage_ref_u), i.e. (f - w_d) - shift_h[d] in f32; zero
+    // for the other storages.
+    float shift_h[Q];
 };
 
 // np.maximum(rho, 1e-30): NaN propagates.
@@ -115,29 +119,45 @@ __device__ __forceinline__ float rho_safe(float r) { return r != r ? r : (r > 1e
 // ---------------------------------------------------------------------------
 // Storage loads / stores
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float ld_dev(const float* p, int d) { return __ldg(p) - wf(d); }
-__device__ __forceinline__ float ld_dev(const __half* p, int) { return __half2float(__ldg(p)); }
-__device__ __forceinline__ float ld_dev(const __nv_bfloat16* p, int) { return __bfloat162float(__ldg(p)); }
+// Loads of population values.  CG = false: the read-only (non-coherent) path,
+// for kernels whose source buffer does not change while they run; CG = true:
+// cached in L2 only (coherent), for the persistent kernel, whose blocks read
+// what other blocks wrote in its previous step.
+template <bool CG, class V>
+__device__ __forceinline__ V ld_pop(const V* p)
+{
+    if constexpr (CG) return __ldcg(p);
+    else return __ldg(p);
+}
+template <bool CG = false>
+__device__ __forceinline__ float ld_dev(const float* p, int d) { return ld_pop<CG>(p) - wf(d); }
+template <bool CG = false>
+__device__ __forceinline__ float ld_dev(const __half* p, int) { return __half2float(ld_pop<CG>(p)); }
+template <bool CG = false>
+__device__ __forceinline__ float ld_dev(const __nv_bfloat16* p, int) { return __bfloat162float(ld_pop<CG>(p)); }
 __device__ __forceinline__ void st_dev(float* p, int d, float h) { *p = h + wf(d); }
 __device__ __forceinline__ void st_dev(__half* p, int, float h) { *p = __float2half_rn(h); }
 __device__ __forceinline__ void st_dev(__nv_bfloat16* p, int, float h) { *p = __float2bfloat16_rn(h); }
 // Two consecutive elements (z, z+1) at an 8-byte (f32) / 4-byte (16-bit)
 // aligned address, as deviations from the weight.
+template <bool CG = false>
 __device__ __forceinline__ void ld_dev2(const float* p, int d, float& a, float& b)
 {
-    const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+    const float2 v = ld_pop<CG>(reinterpret_cast<const float2*>(p));
     a = v.x - wf(d);
     b = v.y - wf(d);
 }
+template <bool CG = false>
 __device__ __forceinline__ void ld_dev2(const __half* p, int, float& a, float& b)
 {
-    const float2 v = __half22float2(__ldg(reinterpret_cast<const __half2*>(p)));
+    const float2 v = __half22float2(ld_pop<CG>(reinterpret_cast<const __half2*>(p)));
     a = v.x;
     b = v.y;
 }
+template <bool CG = false>
 __device__ __forceinline__ void ld_dev2(const __nv_bfloat16* p, int, float& a, float& b)
 {
-    const float2 v = __bfloat1622float2(__ldg(reinterpret_cast<const __nv_bfloat162*>(p)));
+    const float2 v = __bfloat1622float2(ld_pop<CG>(reinterpret_cast<const __nv_bfloat162*>(p)));
     a = v.x;
     b = v.y;
 }
@@ -181,10 +201,10 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __
 
 // Two scalar population values (cells z, z + 1 of one direction, stored at
 // unrelated addresses) as deviations.
-template <class T>
+template <bool CG = false, class T>
 __device__ __forceinline__ float2 ld_dev_pair(const T* pa, const T* pb, int d)
 {
-    return make_float2(ld_dev(pa, d), ld_dev(pb, d));
+    return make_float2(ld_dev<CG>(pa, d), ld_dev<CG>(pb, d));
 }
 
 // f64 value -> storage, rounding as the oracle's store_round does.
@@ -192,22 +212,22 @@ __device__ __forceinline__ void st_f64(double* p, int, double v, const Params&) 
 __device__ __forceinline__ void st_f64(float* p, int, double v, const Params&) { *p = (float)v; }
 __device__ __forceinline__ void st_f64(__half* p, int d, double v, const Params& P)
 {
-    *p = __float2half_rn((float)(v - P.w[d]));
+    *p = __float2half_rn((float)(v - P.w[d]) - P.shift_h[d]);
 }
 __device__ __forceinline__ void st_f64(__nv_bfloat16* p, int d, double v, const Params& P)
 {
-    *p = __float2bfloat16_rn((float)(v - P.w[d]));
+    *p = __float2bfloat16_rn((float)(v - P.w[d]) - P.shift_h[d]);
 }
 // storage -> f64 value
 __device__ __forceinline__ double ld_f64(const double* p, int, const Params&) { return *p; }
 __device__ __forceinline__ double ld_f64(const float* p, int, const Params&) { return (double)*p; }
 __device__ __forceinline__ double ld_f64(const __half* p, int d, const Params& P)
 {
-    return P.w[d] + (double)__half2float(*p);
+    return P.w[d] + (double)(__half2float(*p) + P.shift_h[d]);
 }
 __device__ __forceinline__ double ld_f64(const __nv_bfloat16* p, int d, const Params& P)
 {
-    return P.w[d] + (double)__bfloat162float(*p);
+    return P.w[d] + (double)(__bfloat162float(*p) + P.shift_h[d]);
 }
 
 // ---------------------------------------------------------------------------
@@ -256,12 +276,14 @@ __device__ __forceinline__ void force_fast(const Params& P, int cell, float mx, 
 // ---------------------------------------------------------------------------
 // ModeExact: f64, reference operation order
 // ---------------------------------------------------------------------------
-struct ModeExact {
+template <bool CG = false>
+struct ModeExactT {
     using T = double;
     using C = double;
+    static constexpr bool cg = CG;
 
-    static __device__ __forceinline__ C load(const T* p, int) { return __ldg(p); }
-    static __device__ __forceinline__ void store(T* p, int, C v) { *p = v; }
+    static __device__ __forceinline__ C load(const Params&, const T* p, int) { return ld_pop<CG>(p); }
+    static __device__ __forceinline__ void store(const Params&, T* p, int, C v) { *p = v; }
     static __device__ __forceinline__ C solid(const Params& P, int d) { return P.w[d]; }
     static __device__ __forceinline__ C inflow(const Params& P, int d) { return P.inflow_f[d]; }
     static __device__ __forceinline__ double to_f64(const Params&, int, C v) { return v; }
@@ -381,17 +403,41 @@ struct ModeExact {
     }
     static constexpr bool mass_is_deviation = false;
 };
+using ModeExact = ModeExactT<false>;
 
 // ---------------------------------------------------------------------------
 // ModeFast<T>: f32 arithmetic on deviations h = f - w
 // ---------------------------------------------------------------------------
-template <class TT>
+template <class TT, bool CG = false>
 struct ModeFast {
     using T = TT;
     using C = float;
+    static constexpr bool cg = CG;
 
-    static __device__ __forceinline__ C load(const T* p, int d) { return ld_dev(p, d); }
-    static __device__ __forceinline__ void store(T* p, int d, C h) { st_dev(p, d, h); }
+    // Storage <-> deviation h = f - w: f32 storage holds f itself; the 16-bit
+    // storages hold h - shift_h[d] (the deviation from feq(1, storage_ref_u)).
+    static __device__ __forceinline__ C load(const Params& P, const T* p, int d)
+    {
+        if constexpr (sizeof(TT) == 2) return ld_dev<CG>(p, d) + P.shift_h[d];
+        else return ld_dev<CG>(p, d);
+    }
+    static __device__ __forceinline__ void store(const Params& P, T* p, int d, C h)
+    {
+        if constexpr (sizeof(TT) == 2) st_dev(p, d, h - P.shift_h[d]);
+        else st_dev(p, d, h);
+    }
+    // The same shift for a packed pair (cells z, z + 1) as loaded / to be
+    // stored (scalar adds: the shift is a kernel-parameter operand).
+    static __device__ __forceinline__ float2 unshift2(const Params& P, int d, float2 v)
+    {
+        if constexpr (sizeof(TT) == 2) return make_float2(v.x + P.shift_h[d], v.y + P.shift_h[d]);
+        else return v;
+    }
+    static __device__ __forceinline__ float2 shift2(const Params& P, int d, float2 h)
+    {
+        if constexpr (sizeof(TT) == 2) return make_float2(h.x - P.shift_h[d], h.y - P.shift_h[d]);
+        else return h;
+    }
     static __device__ __forceinline__ C solid(const Params&, int) { return 0.0f; }
     static __device__ __forceinline__ C inflow(const Params& P, int d) { return P.inflow_h[d]; }
     // The f64 population a stored deviation stands for: f32 storage holds
@@ -678,10 +724,10 @@ struct Lane {
 
 // Raw pull of all 19 directions at the position described by nb.
 template <class M, class F>
-__device__ __forceinline__ void gather(const Streams<typename M::T>& S, const Nbr& nb, F&& f)
+__device__ __forceinline__ void gather(const Params& P, const Streams<typename M::T>& S, const Nbr& nb, F&& f)
 {
 #pragma unroll
-    for (int d = 0; d < Q; ++d) f[d] = M::load(S.src[d] + nb.src(d), d);
+    for (int d = 0; d < Q; ++d) f[d] = M::load(P, S.src[d] + nb.src(d), d);
 }
 
 // Replace the pulled values that a boundary rule overrides.  Replacement
@@ -703,9 +749,9 @@ __device__ __forceinline__ void boundary_fix(const Params& P, const Streams<type
         const int face = face_cell ? crossed_face(P, d, gx, y, z) : -1;
         const int o = opp(d);
         if (face >= 0) {
-            f[d] = M::load(S.src[o] + nb.src(o), o) + M::inject(P, face, d, rho_w);
+            f[d] = M::load(P, S.src[o] + nb.src(o), o) + M::inject(P, face, d, rho_w);
         } else if ((bbmask >> d) & 1u) {
-            f[d] = M::load(S.src[o] + gidx, o);
+            f[d] = M::load(P, S.src[o] + gidx, o);
         }
     }
 }
@@ -746,7 +792,7 @@ __device__ __forceinline__ bool resolve_state(const Params& P, const Streams<typ
             return true;
         }
         const Nbr nb2 = make_nbr(P, gx, y, z);
-        gather<M>(S, nb2, f);
+        gather<M>(P, S, nb2, f);
         const bool face2 = on_walled_face(P, gx, y, z);
         const uint32_t m = (g & FLAG_NEAR_SOLID) ? P.bbmask[gidx] & CW_MASK_BITS : 0u;
         if (face2 || m) boundary_fix<M>(P, S, nb2, gx, y, z, gidx, face2, m, f);

@@ -64,6 +64,19 @@ cudaError_t launch_exact(int kernel, int force_mode, const LaunchArgs& a)
     }
 }
 
+cudaError_t launch_persistent_exact(int force_mode, const LaunchArgs& a, int steps, GridBarrier* bar,
+                                    unsigned missing, unsigned long long timeout_ns, int* grid_out)
+{
+    using M = ModeExactT<true>;
+    switch (force_mode) {
+    case FORCE_NONE: return persistent_t<M, FORCE_NONE, 1>(a, steps, bar, missing, timeout_ns, grid_out);
+    case FORCE_UNIFORM: return persistent_t<M, FORCE_UNIFORM, 1>(a, steps, bar, missing, timeout_ns, grid_out);
+    case FORCE_FIELD: return persistent_t<M, FORCE_FIELD, 1>(a, steps, bar, missing, timeout_ns, grid_out);
+    case FORCE_DRAG: return persistent_t<M, FORCE_DRAG, 1>(a, steps, bar, missing, timeout_ns, grid_out);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
 // Batched step, f64 storage (one cell per thread).
 template <int FM>
 static cudaError_t batch_exact_fm(bool collide, const void* records, const void* items, int nitems, int span,
@@ -232,6 +245,135 @@ cudaError_t launch_plane_copy(void* base, size_t dir_stride, size_t plane_off, s
         k_plane_copy<unsigned short><<<grid, block, 0, s>>>((char*)base, dir_stride, plane_off, words, dirs,
                                                             (char*)buf, get);
     }
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Tier-1 / Tier-2 diagnostics of a rho / u readback on the device
+// (Stack-E sim.py:89-109), built --fmad=false so that every value matches
+// the reference's NumPy expressions bit for bit (the circulation sum only up
+// to its summation order).
+// ---------------------------------------------------------------------------
+
+// NumPy's min / max: a NaN anywhere gives NaN.
+__device__ __forceinline__ double np_min(double a, double b) { return (a != a || b != b) ? nan("") : (b < a ? b : a); }
+__device__ __forceinline__ double np_max(double a, double b) { return (a != a || b != b) ? nan("") : (b > a ? b : a); }
+
+constexpr int DIAG_BLOCK = 256;
+constexpr int DIAG_VALUES = 6;  // non-finite count, rho min, rho max, max |u|^2, max |div|, sum u_x (z = 0)
+
+// Block reduction with op (identity: op's neutral value); the result is
+// valid in thread 0.  Fixed order: deterministic for a fixed launch shape.
+template <class OP>
+__device__ __forceinline__ double block_reduce(double v, OP op, double identity, double* red)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = op(v, __shfl_down_sync(0xffffffffu, v, o));
+    __syncthreads();  // red[] of an earlier call has been read
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        v = lane < (int)(blockDim.x >> 5) ? red[lane] : identity;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = op(v, __shfl_down_sync(0xffffffffu, v, o));
+    }
+    return v;
+}
+
+struct OpMin { __device__ double operator()(double a, double b) const { return np_min(a, b); } };
+struct OpMax { __device__ double operator()(double a, double b) const { return np_max(a, b); } };
+struct OpSum { __device__ double operator()(double a, double b) const { return a + b; } };
+
+// Per-block partials over a grid-stride share of the cells.  u_max uses
+// sqrt(max s) = max sqrt(s) (sqrt is monotonic and correctly rounded).
+__global__ void __launch_bounds__(DIAG_BLOCK) k_diag_partials(Params P, const double* __restrict__ rho,
+                                                              const double* __restrict__ u, double inv_2dx,
+                                                              double* __restrict__ partials)
+{
+    __shared__ double red[32];
+    double bad = 0.0, rmin = 1.0 / 0.0, rmax = -1.0 / 0.0, smax = -1.0 / 0.0, dmax = 0.0, usum = 0.0;
+    const int n = P.n;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+        const double r = rho[idx], ux = u[idx], uy = u[n + idx], uz = u[2 * n + idx];
+        bad += (isfinite(r) && isfinite(ux) && isfinite(uy) && isfinite(uz)) ? 0.0 : 1.0;
+        rmin = np_min(rmin, r);
+        rmax = np_max(rmax, r);
+        smax = np_max(smax, (ux * ux + uy * uy) + uz * uz);
+    }
+    // z = 0 slice: central differences with periodic wrap in x and y
+    const int slice = P.nx * P.ny;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < slice; k += gridDim.x * blockDim.x) {
+        const int x = k / P.ny, y = k - x * P.ny;
+        const int xp = x + 1 == P.nx ? 0 : x + 1, xm = x == 0 ? P.nx - 1 : x - 1;
+        const int yp = y + 1 == P.ny ? 0 : y + 1, ym = y == 0 ? P.ny - 1 : y - 1;
+        const double* ux = u;
+        const double* uy = u + n;
+        const double div = (ux[(xp * P.ny + y) * P.nz] - ux[(xm * P.ny + y) * P.nz]) * inv_2dx +
+                           (uy[(x * P.ny + yp) * P.nz] - uy[(x * P.ny + ym) * P.nz]) * inv_2dx;
+        dmax = np_max(dmax, fabs(div));
+        usum += ux[(x * P.ny + y) * P.nz];
+    }
+    double* out = partials + (size_t)blockIdx.x * DIAG_VALUES;
+    double v;
+    v = block_reduce(bad, OpSum{}, 0.0, red);
+    if (threadIdx.x == 0) out[0] = v;
+    v = block_reduce(rmin, OpMin{}, 1.0 / 0.0, red);
+    if (threadIdx.x == 0) out[1] = v;
+    v = block_reduce(rmax, OpMax{}, -1.0 / 0.0, red);
+    if (threadIdx.x == 0) out[2] = v;
+    v = block_reduce(smax, OpMax{}, -1.0 / 0.0, red);
+    if (threadIdx.x == 0) out[3] = v;
+    v = block_reduce(dmax, OpMax{}, 0.0, red);
+    if (threadIdx.x == 0) out[4] = v;
+    v = block_reduce(usum, OpSum{}, 0.0, red);
+    if (threadIdx.x == 0) out[5] = v;
+}
+
+// The block partials -> {check_health, rho_min, rho_max, u_max_lat,
+// check_divergence_free, check_circulation} (one block, fixed order).
+__global__ void __launch_bounds__(DIAG_BLOCK) k_diag_final(const double* __restrict__ partials, int nblocks,
+                                                           double dx, double* __restrict__ out6)
+{
+    __shared__ double red[32];
+    double acc[DIAG_VALUES] = {0.0, 1.0 / 0.0, -1.0 / 0.0, -1.0 / 0.0, 0.0, 0.0};
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+        const double* p = partials + (size_t)b * DIAG_VALUES;
+        acc[0] += p[0];
+        acc[1] = np_min(acc[1], p[1]);
+        acc[2] = np_max(acc[2], p[2]);
+        acc[3] = np_max(acc[3], p[3]);
+        acc[4] = np_max(acc[4], p[4]);
+        acc[5] += p[5];
+    }
+    const double bad = block_reduce(acc[0], OpSum{}, 0.0, red);
+    const double rmin = block_reduce(acc[1], OpMin{}, 1.0 / 0.0, red);
+    const double rmax = block_reduce(acc[2], OpMax{}, -1.0 / 0.0, red);
+    const double smax = block_reduce(acc[3], OpMax{}, -1.0 / 0.0, red);
+    const double dmax = block_reduce(acc[4], OpMax{}, 0.0, red);
+    const double usum = block_reduce(acc[5], OpSum{}, 0.0, red);
+    if (threadIdx.x == 0) {
+        out6[0] = bad > 0.0 ? 1.0 : 0.0;
+        out6[1] = rmin;
+        out6[2] = rmax;
+        out6[3] = sqrt(smax);
+        out6[4] = dmax;
+        out6[5] = usum * dx * dx;
+    }
+}
+
+int diag_grid(int n)
+{
+    const int g = (n + DIAG_BLOCK - 1) / DIAG_BLOCK;
+    return g < DIAG_MAX_BLOCKS ? g : DIAG_MAX_BLOCKS;
+}
+
+cudaError_t launch_diagnostics(const Params& P, const double* rho, const double* u, double dx_phys, double* scratch,
+                               double* out6, cudaStream_t s)
+{
+    const int grid = diag_grid(P.n);
+    k_diag_partials<<<grid, DIAG_BLOCK, 0, s>>>(P, rho, u, 0.5 / dx_phys, scratch);
+    k_diag_final<<<1, DIAG_BLOCK, 0, s>>>(scratch, grid, dx_phys, out6);
     return cudaGetLastError();
 }
 

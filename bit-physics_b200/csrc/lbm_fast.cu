@@ -6,8 +6,49 @@
 
 namespace lbm {
 
+__global__ void k_list_rule_quads(Params P, int* __restrict__ list, int* __restrict__ count)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int idx0 = 4 * q;
+    if (idx0 >= P.n) return;
+    int x, y, z0;
+    decode_xyz(P, idx0, x, y, z0);
+    const uint32_t fl4 = P.has_flags ? *reinterpret_cast<const uint32_t*>(P.flags + idx0) : 0u;
+    if (fl4 != 0u || quad_on_walled_face(P, x, y, z0)) list[atomicAdd(count, 1)] = q;
+}
+
+cudaError_t launch_list_rule_quads(const Params& P, int* list, int* count, cudaStream_t s)
+{
+    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    k_list_rule_quads<<<grid_for(P.n / 4, 256), 256, 0, s>>>(P, list, count);
+    return cudaGetLastError();
+}
+
+// k_step4 on the launch stream and, when the lattice has rule quads,
+// k_step4_rules on the side stream between a fork and a join event (the two
+// write disjoint cells and only read the source buffer).
+template <class M, int FM>
+static cudaError_t launch_step4(const LaunchArgs& a, const Streams<typename M::T>& S)
+{
+    cudaError_t e = cudaSuccess;
+    if (a.rule_count > 0) {
+        if ((e = cudaEventRecord(a.fork, a.stream)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(a.side, a.fork, 0)) != cudaSuccess) return e;
+        k_step4_rules<M, FM><<<grid_for(2LL * a.rule_count, 128), 128, 0, a.side>>>(a.P, S, a.rule_quads,
+                                                                                   a.rule_count);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(a.join, a.side)) != cudaSuccess) return e;
+    }
+    const int block = a.block < 128 ? a.block : 128;  // the kernel's bound
+    k_step4<M, FM><<<grid_for(a.P.n / 4, block), block, 0, a.stream>>>(a.P, S);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (a.rule_count > 0) e = cudaStreamWaitEvent(a.stream, a.join, 0);
+    return e;
+}
+
 template <class M, int FM, int OUT>
-static void launch_step_out(int kernel, const LaunchArgs& a, int grid)
+static cudaError_t launch_step_out(int kernel, const LaunchArgs& a, int grid)
 {
     using T = typename M::T;
     Outputs<float> out{(float*)a.rho, (float*)a.u, a.partials, a.prev_partials, a.prev_count, a.prev_sums};
@@ -16,29 +57,32 @@ static void launch_step_out(int kernel, const LaunchArgs& a, int grid)
         if (kernel == KERNEL_STEP && a.vec == 2 && a.pipe_grid > 0) {
             k_step2_pipe<M, FM><<<a.pipe_grid, a.block, 0, a.stream>>>(a.P, S);
             if (a.grid_used) *a.grid_used = a.pipe_grid;
-            return;
+            return cudaGetLastError();
         }
+        if (kernel == KERNEL_STEP && a.vec == 4) return launch_step4<M, FM>(a, S);
     }
+    // Steps with readback or sums of a four-cell lattice run the two-cell kernels.
     if constexpr (OUT == OUT_SUMS) {
-        if (kernel == KERNEL_STEP && a.vec == 2 && a.sums_grid > 0) {
+        if (kernel == KERNEL_STEP && a.vec >= 2 && a.sums_grid > 0) {
             k_step2_sums<M, FM><<<a.sums_grid, a.block, 0, a.stream>>>(a.P, S, out);
             if (a.grid_used) *a.grid_used = a.sums_grid;
-            return;
+            return cudaGetLastError();
         }
     }
-    if (kernel == KERNEL_STEP && a.vec == 2) {
+    if (kernel == KERNEL_STEP && a.vec >= 2) {
         // at most the kernel's bound (128 threads for 16-bit storage)
         const int block = a.block < Step2Bounds<T>::threads ? a.block : Step2Bounds<T>::threads;
         const int grid2 = grid_for(a.P.n / 2, block);
         k_step2<M, FM, OUT><<<grid2, block, 0, a.stream>>>(a.P, S, out);
         if (a.grid_used) *a.grid_used = grid2;
-        return;
+        return cudaGetLastError();
     }
     if (kernel == KERNEL_STEP)
         k_step<M, FM, OUT><<<grid, a.block, 0, a.stream>>>(a.P, S, out);
     else
         k_collide_local<M, FM, OUT><<<grid, a.block, 0, a.stream>>>(a.P, S, out);
     if (a.grid_used) *a.grid_used = grid;
+    return cudaGetLastError();
 }
 
 template <class T, int FM>
@@ -55,14 +99,14 @@ static cudaError_t launch_fast_t(int kernel, const LaunchArgs& a)
         return cudaGetLastError();
     }
     if (kernel != KERNEL_STEP && kernel != KERNEL_COLLIDE_LOCAL) return cudaErrorInvalidValue;
-    if (a.vec == 2 && (a.P.nz % 2) != 0) return cudaErrorInvalidValue;
+    if ((a.vec == 2 && (a.P.nz % 2) != 0) || (a.vec == 4 && (a.P.nz % 4 != 0 || sizeof(T) != 2)))
+        return cudaErrorInvalidValue;
     switch (out_bits(a)) {
-    case OUT_NONE: launch_step_out<M, FM, OUT_NONE>(kernel, a, grid); break;
-    case OUT_RHO_U: launch_step_out<M, FM, OUT_RHO_U>(kernel, a, grid); break;
-    case OUT_SUMS: launch_step_out<M, FM, OUT_SUMS>(kernel, a, grid); break;
+    case OUT_NONE: return launch_step_out<M, FM, OUT_NONE>(kernel, a, grid);
+    case OUT_RHO_U: return launch_step_out<M, FM, OUT_RHO_U>(kernel, a, grid);
+    case OUT_SUMS: return launch_step_out<M, FM, OUT_SUMS>(kernel, a, grid);
     default: return cudaErrorInvalidValue;
     }
-    return cudaGetLastError();
 }
 
 template <class T>
@@ -195,6 +239,43 @@ static int loop_grid(bool sums, int storage, int force_mode, int block)
 int pipe_grid_fast(int storage, int force_mode, int block) { return loop_grid(false, storage, force_mode, block); }
 
 int sums_grid_fast(int storage, int force_mode, int block) { return loop_grid(true, storage, force_mode, block); }
+
+template <class T, int FM>
+static cudaError_t persistent_fm_t(const LaunchArgs& a, int steps, GridBarrier* bar, unsigned missing,
+                                   unsigned long long timeout_ns, int* grid_out)
+{
+    if (a.vec >= 2) return persistent_t<ModeFast<T, true>, FM, 2>(a, steps, bar, missing, timeout_ns, grid_out);
+    return persistent_t<ModeFast<T, true>, FM, 1>(a, steps, bar, missing, timeout_ns, grid_out);
+}
+
+template <class T>
+static cudaError_t persistent_fast_t(int force_mode, const LaunchArgs& a, int steps, GridBarrier* bar,
+                                     unsigned missing, unsigned long long timeout_ns, int* grid_out)
+{
+    switch (force_mode) {
+    case FORCE_NONE: return persistent_fm_t<T, FORCE_NONE>(a, steps, bar, missing, timeout_ns, grid_out);
+    case FORCE_UNIFORM: return persistent_fm_t<T, FORCE_UNIFORM>(a, steps, bar, missing, timeout_ns, grid_out);
+    case FORCE_FIELD: return persistent_fm_t<T, FORCE_FIELD>(a, steps, bar, missing, timeout_ns, grid_out);
+    case FORCE_DRAG: return persistent_fm_t<T, FORCE_DRAG>(a, steps, bar, missing, timeout_ns, grid_out);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_persistent_exact(int force_mode, const LaunchArgs& a, int steps, GridBarrier* bar,
+                                    unsigned missing, unsigned long long timeout_ns, int* grid_out);
+
+cudaError_t launch_persistent(int storage, int force_mode, const LaunchArgs& a, int steps, GridBarrier* bar,
+                              unsigned missing, unsigned long long timeout_ns, int* grid_out)
+{
+    switch (storage) {
+    case STORAGE_F64: return launch_persistent_exact(force_mode, a, steps, bar, missing, timeout_ns, grid_out);
+    case STORAGE_F32: return persistent_fast_t<float>(force_mode, a, steps, bar, missing, timeout_ns, grid_out);
+    case STORAGE_F16: return persistent_fast_t<__half>(force_mode, a, steps, bar, missing, timeout_ns, grid_out);
+    case STORAGE_BF16:
+        return persistent_fast_t<__nv_bfloat16>(force_mode, a, steps, bar, missing, timeout_ns, grid_out);
+    default: return cudaErrorInvalidValue;
+    }
+}
 
 cudaError_t launch_fast(int storage, int kernel, int force_mode, const LaunchArgs& a)
 {

@@ -31,6 +31,7 @@ struct lbm_lattice {
     int partial_blocks = 0;  // rows of partials of one launch (one per block, any kernel)
     double* staging = nullptr; // (19, n) f64, allocated on first use
     double* monitor = nullptr; // (monitor_cap, 5) per-step sums of lbm_step_monitor
+    double* diag = nullptr;    // DIAG_SCRATCH + 6 doubles of lbm_diagnostics, allocated on first use
     int monitor_cap = 0;
     int64_t steps = 0;
     int block = 256;
@@ -46,6 +47,19 @@ struct lbm_lattice {
     int tma_grid = 0;
     int pipe_grid = 0;  // > 0: steps without outputs run k_step2_pipe
     int sums_grid = 0;  // > 0: steps with FP64 sums run k_step2_sums
+    // Four-cell steps (vec == 4): the quads that need a boundary rule, stepped
+    // by k_step4_rules on a second stream beside k_step4.
+    int* rule_quads = nullptr;  // (n / 4 + 1): the list, then its length
+    int rule_count = 0;
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // Many steps per cooperative launch (LBM_STAGING_PERSISTENT): barrier
+    // state, the limit of one barrier wait, and arrivals added to the
+    // expected count (nonzero only through lbm_test_barrier_limit).
+    bool persist = false;
+    lbm::GridBarrier* bar = nullptr;
+    unsigned long long persist_timeout_ns = 2000000000ull;
+    unsigned persist_missing = 0;
     lbm::TileCfg tile{};
     lbm::Params P{};
 };

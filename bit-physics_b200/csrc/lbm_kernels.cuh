@@ -127,17 +127,28 @@ __device__ __forceinline__ void emit(const Params& P, const Outputs<typename M::
 }
 
 template <class M>
-__device__ __forceinline__ void store_all(const Streams<typename M::T>& S, int idx, const typename M::C* f)
+__device__ __forceinline__ void store_all(const Params& P, const Streams<typename M::T>& S, int idx,
+                                          const typename M::C* f)
 {
 #pragma unroll
-    for (int d = 0; d < Q; ++d) M::store(S.dst[d] + idx, d, f[d]);
+    for (int d = 0; d < Q; ++d) M::store(P, S.dst[d] + idx, d, f[d]);
 }
 
 template <class M>
 __device__ __forceinline__ void store_solid(const Params& P, const Streams<typename M::T>& S, int idx)
 {
 #pragma unroll
-    for (int d = 0; d < Q; ++d) M::store(S.dst[d] + idx, d, M::solid(P, d));
+    for (int d = 0; d < Q; ++d) M::store(P, S.dst[d] + idx, d, M::solid(P, d));
+}
+
+// Post-collision direction d of a pair (cells idx0, idx0 + 1 of one row) as
+// one vector store; a solid cell stores its rest state.
+template <class M>
+__device__ __forceinline__ void store_pair(const Params& P, const Streams<typename M::T>& S, int idx0, int d,
+                                           float2 v, bool fluid0, bool fluid1)
+{
+    const float2 s = M::shift2(P, d, make_float2(fluid0 ? v.x : M::solid(P, d), fluid1 ? v.y : M::solid(P, d)));
+    st_dev2(S.dst[d] + idx0, d, s.x, s.y);
 }
 
 // Fused step from POST for one cell: f_n = gather + resolve_state(P_{n-1});
@@ -154,11 +165,11 @@ __device__ __forceinline__ void step_single(const Params& P, const Streams<typen
     const int fl = P.has_flags ? (int)P.flags[idx] : 0;
     const Nbr nb = make_nbr(P, x, y, z);
     C f[Q];
-    gather<M>(S, nb, f);
+    gather<M>(P, S, nb, f);
     if (resolve_state<M>(P, S, idx, x, y, z, fl, nb, f)) {
         emit<M, FM, OUT>(P, out, idx, false, f, cons);
         M::template collide<FM>(P, idx, f);
-        store_all<M>(S, idx, f);
+        store_all<M>(P, S, idx, f);
     } else {
         emit<M, FM, OUT>(P, out, idx, true, f, cons);
         store_solid<M>(P, S, idx);
@@ -182,20 +193,21 @@ __global__ void __launch_bounds__(256, 3) k_step(Params P, Streams<typename M::T
 // Plain pull gather of the pair (x, y, z0), (x, y, z0 + 1) described by nb
 // (zp1 = z0 + 2, wrapped): the c_z = 0 directions as one vector load.
 template <class M>
-__device__ __forceinline__ void gather_pair(const Streams<typename M::T>& S, const Nbr& nb, int z0, int zp1,
-                                            float2* h)
+__device__ __forceinline__ void gather_pair(const Params& P, const Streams<typename M::T>& S, const Nbr& nb, int z0,
+                                            int zp1, float2* h)
 {
     using T = typename M::T;
 #pragma unroll
     for (int d = 0; d < Q; ++d) {
         const T* p = S.src[d] + nb.X[1 - cx(d)] + nb.Y[1 - cy(d)];
         if (cz(d) == 0) {
-            ld_dev2(p + z0, d, h[d].x, h[d].y);
+            ld_dev2<M::cg>(p + z0, d, h[d].x, h[d].y);
         } else if (cz(d) == 1) {
-            h[d] = ld_dev_pair(p + nb.Z[0], p + z0, d);
+            h[d] = ld_dev_pair<M::cg>(p + nb.Z[0], p + z0, d);
         } else {
-            h[d] = ld_dev_pair(p + z0 + 1, p + zp1, d);
+            h[d] = ld_dev_pair<M::cg>(p + z0 + 1, p + zp1, d);
         }
+        h[d] = M::unshift2(P, d, h[d]);
     }
 }
 
@@ -233,8 +245,8 @@ __device__ __forceinline__ void resolve_pair(const Params& P, const Streams<type
 #pragma unroll
             for (int d = 1; d < Q; ++d) {
                 const int o = opp(d);
-                if ((m0 >> d) & 1u) h[d].x = M::load(S.src[o] + idx0, o);
-                if ((m1 >> d) & 1u) h[d].y = M::load(S.src[o] + idx0 + 1, o);
+                if ((m0 >> d) & 1u) h[d].x = M::load(P, S.src[o] + idx0, o);
+                if ((m1 >> d) & 1u) h[d].y = M::load(P, S.src[o] + idx0 + 1, o);
             }
         }
         return;
@@ -253,7 +265,7 @@ __device__ __forceinline__ void resolve_pair(const Params& P, const Streams<type
         if ((g0 & 3) == CELL_OUTFLOW) g0 &= ~3;
         if ((g1 & 3) == CELL_OUTFLOW) g1 &= ~3;
         if ((g0 | g1) == 0 && !on_walled_face(P, gx, y, z0) && !on_walled_face(P, gx, y, z0 + 1)) {
-            gather_pair<M>(S, make_nbr(P, gx, y, z0), z0, zp1, h);
+            gather_pair<M>(P, S, make_nbr(P, gx, y, z0), z0, zp1, h);
             fluid0 = fluid1 = true;
             return;
         }
@@ -301,7 +313,7 @@ __device__ __forceinline__ void step_pair(const Params& P, const Streams<typenam
     const Nbr nb0 = make_nbr(P, x, y, z0);
     const int zp1 = z0 + 2 == P.nz ? 0 : z0 + 2; // (z0 + 1) + 1, wrapped
     float2 h[Q];
-    gather_pair<M>(S, nb0, z0, zp1, h);
+    gather_pair<M>(P, S, nb0, z0, zp1, h);
     bool fluid0 = true, fluid1 = true;
     const bool face = on_walled_face(P, x, y, z0) || on_walled_face(P, x, y, z0 + 1);
     if ((fl0 | fl1 | (int)face) != 0)
@@ -316,7 +328,7 @@ __device__ __forceinline__ void step_pair(const Params& P, const Streams<typenam
         emit<M, FM, OUT_RHO_U>(P, out, idx0 + 1, !fluid1, f, cons);
     }
     const auto mo = M::template collide2<FM>(P, idx0, h, [&](int d, float2 v) {
-        if (live) st_dev2(S.dst[d] + idx0, d, fluid0 ? v.x : M::solid(P, d), fluid1 ? v.y : M::solid(P, d));
+        if (live) store_pair<M>(P, S, idx0, d, v, fluid0, fluid1);
     });
     if constexpr ((OUT & OUT_SUMS) != 0) {
         // the collision's own pre-collision moments (density deviation,
@@ -348,7 +360,8 @@ __device__ __forceinline__ void step_pair_scalar(const Params& P, const Streams<
     const Nbr nb1 = make_nbr(P, x1, y1, z1);
     float2 h[Q];
 #pragma unroll
-    for (int d = 0; d < Q; ++d) h[d] = ld_dev_pair(S.src[d] + nb0.src(d), S.src[d] + nb1.src(d), d);
+    for (int d = 0; d < Q; ++d)
+        h[d] = M::unshift2(P, d, ld_dev_pair<M::cg>(S.src[d] + nb0.src(d), S.src[d] + nb1.src(d), d));
     bool fluid0 = true, fluid1 = true;
     if ((fl0 | fl1 | (int)on_walled_face(P, x0, y0, z0) | (int)on_walled_face(P, x1, y1, z1)) != 0) {
         fluid0 = resolve_state<M>(P, S, idx0, x0, y0, z0, fl0, nb0, Lane<0>{h});
@@ -359,26 +372,27 @@ __device__ __forceinline__ void step_pair_scalar(const Params& P, const Streams<
     // inputs; the scalar path serves the force-free and uniform models only.
     static_assert(FM == FORCE_NONE || FM == FORCE_UNIFORM, "step_pair_scalar: per-cell forces unsupported");
     M::template collide2<FM>(P, idx0, h, [&](int d, float2 v) {
-        M::store(S.dst[d] + idx0, d, fluid0 ? v.x : M::solid(P, d));
-        if (two) M::store(S.dst[d] + idx1, d, fluid1 ? v.y : M::solid(P, d));
+        M::store(P, S.dst[d] + idx0, d, fluid0 ? v.x : M::solid(P, d));
+        if (two) M::store(P, S.dst[d] + idx1, d, fluid1 ? v.y : M::solid(P, d));
     });
 }
 
 // Launch bounds of k_step2: f32 storage at 3 blocks of 256 per SM (80
-// registers); the 16-bit storages at 5 blocks of 128 (96 registers, 20
-// warps: f16 sphere channel 60.4 against 59.1 GLUPS at 80 registers and
-// 54.6 at 128; f32 at 96 registers ran 38.1 against 40.1).
+// registers); the 16-bit storages at 4 blocks of 128 (128 registers: with the
+// storage reference shift the kernel spilled 252 B per thread at 96).  The
+// 16-bit storages step with k_step4 where nz is a multiple of 4; k_step2
+// serves their readback and sums steps and the other even nz.
 template <class T>
 struct Step2Bounds {
     static constexpr int threads = 256, blocks = LBM_STEP2_MIN_BLOCKS;
 };
 template <>
 struct Step2Bounds<__half> {
-    static constexpr int threads = 128, blocks = 5;
+    static constexpr int threads = 128, blocks = 4;
 };
 template <>
 struct Step2Bounds<__nv_bfloat16> {
-    static constexpr int threads = 128, blocks = 5;
+    static constexpr int threads = 128, blocks = 4;
 };
 
 template <class M, int FM, int OUT>
@@ -515,7 +529,8 @@ __global__ void __launch_bounds__(256, 2) k_step2_pipe(Params P, Streams<typenam
         float2 h[Q];
 #pragma unroll
         for (int d = 0; d < Q; ++d)
-            h[d] = cz(d) == 0 ? word_dev2(r.w[d], T{}) : make_float2(half_dev(r.a[d], T{}), half_dev(r.b[d], T{}));
+            h[d] = M::unshift2(P, d, cz(d) == 0 ? word_dev2(r.w[d], T{})
+                                               : make_float2(half_dev(r.a[d], T{}), half_dev(r.b[d], T{})));
         const int fl0 = (int)(r.cw0 >> CW_FLAG_SHIFT), fl1 = (int)(r.cw1 >> CW_FLAG_SHIFT);
         PairMasks<true> cm;
         cm.m0 = r.cw0 & CW_MASK_BITS;
@@ -531,11 +546,197 @@ __global__ void __launch_bounds__(256, 2) k_step2_pipe(Params P, Streams<typenam
             const int zp1 = z0 + 2 == P.nz ? 0 : z0 + 2;
             resolve_pair<M, true>(P, S, idx0, x, y, z0, fl0, fl1, face, nb0, zp1, h, fluid0, fluid1, cm);
         }
-        M::template collide2<FM>(P, idx0, h, [&](int d, float2 v) {
-            st_dev2(S.dst[d] + idx0, d, fluid0 ? v.x : M::solid(P, d), fluid1 ? v.y : M::solid(P, d));
-        });
+        M::template collide2<FM>(P, idx0, h, [&](int d, float2 v) { store_pair<M>(P, S, idx0, d, v, fluid0, fluid1); });
         if (q >= np) break;
         p = q;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Four-cell step for 16-bit storage
+// ---------------------------------------------------------------------------
+
+// Two values of the 16-bit storage format packed in a 32-bit word (low half:
+// the lower z), rounded as st_dev2 rounds.
+__device__ __forceinline__ uint32_t pack_dev2(float a, float b, __half)
+{
+    const __half2 v = __floats2half2_rn(a, b);
+    uint32_t w;
+    memcpy(&w, &v, sizeof w);
+    return w;
+}
+__device__ __forceinline__ uint32_t pack_dev2(float a, float b, __nv_bfloat16)
+{
+    const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+    uint32_t w;
+    memcpy(&w, &v, sizeof w);
+    return w;
+}
+
+// A quad -- four z-adjacent cells z0..z0 + 3 of one row, z0 a multiple of 4
+// -- is plain when its four cells are fluid, none pulls from a solid cell
+// and none lies on a walled face: its post-stream state is the raw gather.
+__device__ __forceinline__ bool quad_on_walled_face(const Params& P, int x, int y, int z0)
+{
+    return on_walled_face(P, x, y, z0) || on_walled_face(P, x, y, z0 + 3);
+}
+
+// Fused step from POST of the plain quads, four cells per thread, 16-bit
+// storage, nz a multiple of 4: the default step kernel of the 16-bit storages
+// when no readback or sums are asked for.  Every direction is one aligned
+// 8-byte load of the four cells' sources, plus one 2-byte load of the fifth
+// value a z-shifted direction needs; the packed collision runs on cells
+// (z0, z0 + 1), then (z0 + 2, z0 + 3), and each direction leaves as one
+// 8-byte store.  Against the two-cell kernel a thread keeps twice the bytes in
+// flight per load phase and issues fewer instructions per cell: 78.6 against
+// 66.0 GLUPS (f16) on the 256x128x128 lattice without flags, the same results
+// bit for bit.  The quads that need a rule (3.7 % of the sphere channel's)
+// return here and are stepped by k_step4_rules, launched beside this kernel
+// on a second stream: inside this kernel they would hold up their whole
+// warp (the rule quads sit in 23 % of the channel's rows), and their code
+// would raise the register demand of the plain path.  The flag bytes of the
+// quad are one 4-byte load issued with the gather.
+template <class M, int FM>
+__global__ void __launch_bounds__(128, 4) k_step4(Params P, Streams<typename M::T> S)
+{
+    using T = typename M::T;
+    static_assert(sizeof(T) == 2, "k_step4: 16-bit storage only");
+    const int idx0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (idx0 >= P.n) return;
+    int x, y, z0;
+    decode_xyz(P, idx0, x, y, z0);
+    const Nbr nb0 = make_nbr(P, x, y, z0);
+    const int zr = z0 + 4 == P.nz ? 0 : z0 + 4;
+    uint2 raw[Q];
+    uint32_t edge[Q];
+#pragma unroll
+    for (int d = 0; d < Q; ++d) {
+        const unsigned short* p =
+            reinterpret_cast<const unsigned short*>(S.src[d]) + nb0.X[1 - cx(d)] + nb0.Y[1 - cy(d)];
+        raw[d] = __ldg(reinterpret_cast<const uint2*>(p + z0));
+        edge[d] = cz(d) == 1 ? (uint32_t)__ldg(p + nb0.Z[0]) : (cz(d) == -1 ? (uint32_t)__ldg(p + zr) : 0u);
+    }
+    const uint32_t fl4 = P.has_flags ? __ldg(reinterpret_cast<const uint32_t*>(P.flags + idx0)) : 0u;
+    if (fl4 != 0u || quad_on_walled_face(P, x, y, z0)) return;  // a rule quad: k_step4_rules
+    uint32_t lo[Q];  // stored words of cells z0, z0 + 1
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+        float2 h[Q];
+#pragma unroll
+        for (int d = 0; d < Q; ++d) {
+            uint32_t w;
+            if (cz(d) == 0) w = half == 0 ? raw[d].x : raw[d].y;
+            else if (cz(d) == 1) w = half == 0 ? (raw[d].x << 16) | edge[d] : __funnelshift_r(raw[d].x, raw[d].y, 16);
+            else w = half == 0 ? __funnelshift_r(raw[d].x, raw[d].y, 16) : __funnelshift_r(raw[d].y, edge[d], 16);
+            h[d] = M::unshift2(P, d, word_dev2(w, T{}));
+        }
+        M::template collide2<FM>(P, idx0 + 2 * half, h, [&](int d, float2 v) {
+            const float2 sv = M::shift2(P, d, v);
+            const uint32_t w = pack_dev2(sv.x, sv.y, T{});
+            if (half == 0) lo[d] = w;
+            else *reinterpret_cast<uint2*>(S.dst[d] + idx0) = make_uint2(lo[d], w);
+        });
+    }
+}
+
+// The quads of k_step4 that need a boundary rule (quads[0..count) of the
+// lattice's list, launch_list_rule_quads), one pair per thread through the
+// two-cell step.
+template <class M, int FM>
+__global__ void __launch_bounds__(128) k_step4_rules(Params P, Streams<typename M::T> S,
+                                                     const int* __restrict__ quads, int count)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= 2 * count) return;
+    const Outputs<float> none{nullptr, nullptr, nullptr};
+    step_pair<M, FM, OUT_NONE>(P, S, none, 4 * quads[k >> 1] + 2 * (k & 1), nullptr);
+}
+
+// List of the quads that are not plain (order unspecified; each quad's work
+// is independent of the others'); *count on the device.
+__global__ void k_list_rule_quads(Params P, int* __restrict__ list, int* __restrict__ count);
+
+// ---------------------------------------------------------------------------
+// Many steps in one cooperative launch (lattices that fit in L2)
+// ---------------------------------------------------------------------------
+
+// Device state of a grid barrier: arrivals of the current round and the
+// round number; a timed-out wait raises *err (the lattice's error word).
+struct GridBarrier {
+    unsigned count;
+    unsigned gen;
+};
+
+__device__ __forceinline__ unsigned long long global_ns_now()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Barrier over the blocks of a cooperative launch (all co-resident).  Thread
+// 0 of a block counts its arrival; the last of `expected` arrivals resets the
+// count and opens the next round, the others wait for the round to change --
+// for at most timeout_ns, or until another block has raised *err.  Returns
+// false (every thread of the block) when the wait gave up; *err is then set.
+__device__ __forceinline__ bool grid_sync(GridBarrier* b, int* err, unsigned expected,
+                                          unsigned long long timeout_ns)
+{
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        volatile unsigned* gen = &b->gen;
+        volatile int* verr = err;
+        const unsigned g = *gen;
+        __threadfence();
+        if (atomicAdd(&b->count, 1u) == expected - 1u) {
+            atomicExch(&b->count, 0u);
+            __threadfence();
+            atomicAdd(&b->gen, 1u);
+        } else {
+            const unsigned long long t0 = global_ns_now();
+            while (*gen == g) {
+                if (*verr != 0) {
+                    ok = 0;
+                    break;
+                }
+                if (global_ns_now() - t0 > timeout_ns) {
+                    atomicExch(err, 1);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(100);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// `steps` fused steps from POST in one cooperative launch: step s reads
+// S[s & 1].src and writes S[s & 1].dst, every block working through the
+// cells (pairs with VEC = 2) in a grid-stride loop, with a grid barrier
+// between steps.  The per-cell work is that of k_step / k_step2, so the
+// results are the same bits; what goes away is a launch and its tail per
+// step, which dominates lattices small enough to stay in L2.  A barrier wait
+// that runs out (expected arrivals that never come) raises *P.err, and every
+// block leaves at its next barrier.
+template <class M, int FM, int VEC>
+__global__ void __launch_bounds__(256) k_step_persistent(Params P, Streams<typename M::T> S0,
+                                                         Streams<typename M::T> S1, int steps, GridBarrier* bar,
+                                                         unsigned expected, unsigned long long timeout_ns)
+{
+    const Outputs<typename M::C> none{nullptr, nullptr, nullptr};
+    const int items = VEC == 2 ? P.n / 2 : P.n;
+    for (int s = 0; s < steps; ++s) {
+        const Streams<typename M::T>& S = (s & 1) ? S1 : S0;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < items; i += gridDim.x * blockDim.x) {
+            if constexpr (VEC == 2) step_pair<M, FM, OUT_NONE>(P, S, none, 2 * i, nullptr);
+            else step_single<M, FM, OUT_NONE>(P, S, none, i, nullptr);
+        }
+        if (s + 1 < steps && !grid_sync(bar, P.err, expected, timeout_ns)) return;
     }
 }
 
@@ -548,14 +749,14 @@ __device__ __forceinline__ void collide_single(const Params& P, const Streams<ty
     const int type = P.has_flags ? (P.flags[idx] & 3) : CELL_FLUID;
     C f[Q];
 #pragma unroll
-    for (int d = 0; d < Q; ++d) f[d] = M::load(S.src[d] + idx, d);
+    for (int d = 0; d < Q; ++d) f[d] = M::load(P, S.src[d] + idx, d);
     if (type == CELL_SOLID) {
         emit<M, FM, OUT>(P, out, idx, true, f, cons);
         store_solid<M>(P, S, idx);
     } else {
         emit<M, FM, OUT>(P, out, idx, false, f, cons);
         M::template collide<FM>(P, idx, f);
-        store_all<M>(S, idx, f);
+        store_all<M>(P, S, idx, f);
     }
 }
 
@@ -591,7 +792,7 @@ __global__ void __launch_bounds__(256) k_observe(Params P, Streams<typename M::T
             int x, y, z;
             decode_xyz(P, idx, x, y, z);
             const Nbr nb = make_nbr(P, x, y, z);
-            gather<M>(S, nb, f);
+            gather<M>(P, S, nb, f);
             solid = !resolve_state<M>(P, S, idx, x, y, z, fl, nb, f);
             if (solid) {
 #pragma unroll
@@ -600,7 +801,7 @@ __global__ void __launch_bounds__(256) k_observe(Params P, Streams<typename M::T
         } else {
             solid = (fl & 3) == CELL_SOLID;
 #pragma unroll
-            for (int d = 0; d < Q; ++d) f[d] = M::load(S.src[d] + idx, d);
+            for (int d = 0; d < Q; ++d) f[d] = M::load(P, S.src[d] + idx, d);
         }
         if (f_out) {
 #pragma unroll

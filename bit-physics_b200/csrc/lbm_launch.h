@@ -37,6 +37,12 @@ struct LaunchArgs {
                         // k_step2_pipe with this grid
     int sums_grid = 0;  // > 0: a two-cell KERNEL_STEP with partials runs
                         // k_step2_sums with this grid
+    // vec == 4 steps without outputs: the rule quads (k_step4_rules) run on
+    // `side` between the fork and join events
+    const int* rule_quads = nullptr;
+    int rule_count = 0;
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 // Output selection of a step launch (OUT_* bits of lbm_kernels.cuh) from the
@@ -59,7 +65,17 @@ cudaError_t launch_load_f64(int storage, const Params& P, const void* src, doubl
 cudaError_t launch_feq_init(int storage, const Params& P, const double* rho, const double* u, void* dst,
                             cudaStream_t s);
 cudaError_t launch_mark_near_solid(const Params& P, uint8_t* flags, uint32_t* bbmask, cudaStream_t s);
+// The quads of a lattice (nz a multiple of 4) that k_step4 leaves to
+// k_step4_rules, into list; their number into *count (device).
+cudaError_t launch_list_rule_quads(const Params& P, int* list, int* count, cudaStream_t s);
 cudaError_t launch_reduce_partials(const double* partials, int nblocks, double* out5, cudaStream_t s);
+// Tier-1 / Tier-2 diagnostics of f64 rho (n) / u (3, n) device arrays into
+// out6 (device): {check_health, rho_min, rho_max, u_max_lat,
+// check_divergence_free, check_circulation}; scratch: DIAG_SCRATCH doubles.
+constexpr int DIAG_MAX_BLOCKS = 1184;
+constexpr size_t DIAG_SCRATCH = (size_t)DIAG_MAX_BLOCKS * 6;
+cudaError_t launch_diagnostics(const Params& P, const double* rho, const double* u, double dx_phys, double* scratch,
+                               double* out6, cudaStream_t s);
 // x-slab exchange: plane (plane_off bytes into each direction, plane_bytes
 // long, directions dir_stride bytes apart) of the directions in mask to
 // (get) or from the packed buffer, one launch.
@@ -76,6 +92,43 @@ cudaError_t launch_batch_step(int storage, int force_mode, int sched, bool colli
                               const void* items, int nitems, int span, int phase, int grid, int block,
                               cudaStream_t s);
 size_t batch_record_bytes(int storage);
+
+// `steps` steps from POST in one cooperative launch (k_step_persistent;
+// a.src / a.dst: the buffers of the first step, which alternate).  The grid
+// is every block that fits on the device at once; a barrier wait gives up
+// after timeout_ns (raising *a.P.err), and `missing` arrivals are added to
+// the expected count (nonzero only to test that path).  *grid_out: the grid.
+cudaError_t launch_persistent(int storage, int force_mode, const LaunchArgs& a, int steps, GridBarrier* bar,
+                              unsigned missing, unsigned long long timeout_ns, int* grid_out);
+
+// The cooperative launch of k_step_persistent<M, FM, VEC> (see launch_persistent).
+template <class M, int FM, int VEC>
+inline cudaError_t persistent_t(const LaunchArgs& a, int steps, GridBarrier* bar, unsigned missing,
+                         unsigned long long timeout_ns, int* grid_out)
+{
+    using T = typename M::T;
+    auto kern = k_step_persistent<M, FM, VEC>;
+    const int block = 256;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorLaunchOutOfResources;
+    const int items = VEC == 2 ? a.P.n / 2 : a.P.n;
+    int grid = sms * per_sm;
+    const int need = (items + block - 1) / block;
+    if (grid > need) grid = need;  // no block without work
+    Params P = a.P;
+    Streams<T> S0 = make_streams<T>(a.src, a.dst, a.P.n);
+    Streams<T> S1 = make_streams<T>(a.dst, const_cast<void*>(a.src), a.P.n);
+    unsigned expected = (unsigned)grid + missing;
+    void* args[] = {&P, &S0, &S1, &steps, &bar, &expected, &timeout_ns};
+    if ((e = cudaMemsetAsync(bar, 0, sizeof(GridBarrier), a.stream)) != cudaSuccess) return e;
+    e = cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(block), args, 0, a.stream);
+    if (grid_out) *grid_out = grid;
+    return e;
+}
 
 // TMA-staged step (lbm_tma.cu): tile plan for a lattice (stages == 0 when the
 // path does not apply) and the launch.

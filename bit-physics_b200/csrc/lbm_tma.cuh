@@ -223,6 +223,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(Params P, Streams<t
                     if (cz(d) == 0) h[d] = ld_dev2_sm(row + z0, d);
                     else if (cz(d) == 1) h[d] = sm_pair(row, zm, z0, d);
                     else h[d] = sm_pair(row, z0 + 1, zp1, d);
+                    h[d] = M::unshift2(P, d, h[d]);
                 }
                 const int y = y0 + r;
                 bool fluid0 = true, fluid1 = true;
@@ -245,9 +246,8 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(Params P, Streams<t
                     for (int d = 0; d < Q; ++d) f[d] = h[d].y;
                     emit<M, FM, OUT>(P, out, idx0 + 1, !fluid1, f, cons);
                 }
-                M::template collide2<FM>(P, idx0, h, [&](int d, float2 v) {
-                    st_dev2(S.dst[d] + idx0, d, fluid0 ? v.x : M::solid(P, d), fluid1 ? v.y : M::solid(P, d));
-                });
+                M::template collide2<FM>(P, idx0, h,
+                                         [&](int d, float2 v) { store_pair<M>(P, S, idx0, d, v, fluid0, fluid1); });
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[s]);

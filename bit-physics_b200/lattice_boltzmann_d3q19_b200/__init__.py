@@ -12,7 +12,9 @@ package's step and state API:
 * ``Tape``       -- checkpointed forward + hand-written adjoint kernels, and
   ``autograd.run``, its torch.autograd.Function (gradients w.r.t. the
   porosity field and the initial populations);
-* ``sim``        -- the canonical Poiseuille / Couette runners.
+* ``sim``        -- the canonical Poiseuille / Couette runners;
+* ``captures``   -- load / compare captures with the reference's equivalence
+  gate and tolerance, and convert them to its HDF5 capture format.
 """
 
 from __future__ import annotations

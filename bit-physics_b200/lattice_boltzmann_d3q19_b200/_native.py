@@ -27,7 +27,7 @@ LBM_ERR_NO_DEVICE = -7
 STORAGE = {"f64": 0, "f32": 1, "f16": 2, "bf16": 3}
 FORCE = {"none": 0, "uniform": 1, "field": 2, "drag": 3}
 FACES = {"x-": 0, "x+": 1, "y-": 2, "y+": 3, "z-": 4, "z+": 5}
-STAGING = {"auto": 0, "registers": 1, "tma": 2, "pipelined": 3}
+STAGING = {"auto": 0, "registers": 1, "tma": 2, "pipelined": 3, "persistent": 4}
 SCHEDULES = {"single": 0, "pair_scalar": 1, "pair_mixed": 2}
 CELL_FLUID, CELL_SOLID, CELL_INFLOW, CELL_OUTFLOW = 0, 1, 2, 3
 
@@ -58,6 +58,7 @@ class LbmDesc(C.Structure):
         ("block_size", C.c_int32),
         ("cells_per_thread", C.c_int32),
         ("staging", C.c_int32),
+        ("storage_ref_u", C.c_double * 3),
     ]
 
 
@@ -118,6 +119,8 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "lbm_plane_put": ([_h, _i, C.c_uint32, _h], C.c_int),
     "lbm_conservation_planes": ([_h, _i, _i, _dp], C.c_int),
     "lbm_get_rho_u_dev": ([_h, _h, _h], C.c_int),
+    "lbm_diagnostics": ([_h, C.c_double, _dp], C.c_int),
+    "lbm_test_barrier_limit": ([_h, C.c_int32, C.c_int64], C.c_int),
     "lbm_set_porosity_dev": ([_h, _h], C.c_int),
     "lbm_tape_forward": ([_h, _i, _i, C.POINTER(_h)], C.c_int),
     "lbm_tape_backward": ([_h, _h, _h, _h, _h], C.c_int),

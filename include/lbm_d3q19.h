@@ -83,9 +83,15 @@ typedef struct lbm_desc {
     double inflow_u[3];  /* inflow cell velocity                             */
     int32_t device;      /* CUDA device ordinal                              */
     int32_t block_size;  /* threads per block for the step kernels; 0 = auto */
-    int32_t cells_per_thread; /* step kernel: 1, or 2 (f32/f16/bf16 storage with
-                                 nz even); 0 = auto                          */
+    int32_t cells_per_thread; /* step kernel: 1; 2 (f32/f16/bf16 storage,
+                                 nz even); 4 (f16/bf16 storage, nz a
+                                 multiple of 4, register staging); 0 = auto */
     int32_t staging;     /* step kernel input staging: LBM_STAGING_*         */
+    double storage_ref_u[3]; /* f16/bf16 storage: populations are held as the
+                                16-bit deviation from feq(1, storage_ref_u)
+                                (default 0: f - w_i); a reference velocity
+                                near the flow's keeps the deviations small,
+                                so the rounding error is small           */
 } lbm_desc;
 
 /* Step-kernel staging (lbm_desc.staging). */
@@ -99,6 +105,12 @@ typedef struct lbm_desc {
                                    loop): two cells per thread, f16/bf16 storage;
                                    steps with readback or sums run the two-cell
                                    kernel                                         */
+#define LBM_STAGING_PERSISTENT 4 /* lbm_step runs all its steady-state steps in
+                                    one cooperative launch, every block stepping
+                                    its share of the cells and a grid barrier
+                                    between steps (lattices that stay in L2, where
+                                    a launch per step costs more than the step);
+                                    loads of populations cached in L2 only       */
 
 typedef struct lbm_lattice lbm_lattice;
 
@@ -275,6 +287,25 @@ int lbm_tape_backward(lbm_tape* t, const double* grad_rho, const double* grad_u,
 /* Device bytes the tape holds (checkpoints, segment states, adjoint fields). */
 int64_t lbm_tape_bytes(const lbm_tape* t);
 int lbm_tape_destroy(lbm_tape* t);
+
+/* Tier-1 / Tier-2 diagnostics of the current state, reduced on the GPU
+ * (replaces the NumPy diagnostics of Stack-E sim.py:89-109 after a full host
+ * readback): out6 = {check_health (0 all finite, 1 otherwise), rho_min,
+ * rho_max, u_max_lat = max |u|, check_divergence_free = max |div u| on the
+ * z = 0 slice by periodic central differences with spacing dx_phys,
+ * check_circulation = sum of u_x over that slice * dx_phys^2}, of the rho /
+ * u that lbm_get_rho_u would return (solid cells read back as 0).  Equal to
+ * the reference's expressions on those arrays bit for bit, except the
+ * circulation sum's order of summation. */
+int lbm_diagnostics(lbm_lattice* h, double dx_phys, double* out6);
+
+/* Test hook of the persistent step's bounded grid barrier: the next
+ * cooperative launches of h expect `missing_arrivals` more blocks than they
+ * launch (so no barrier opens) and give up each wait after timeout_ns
+ * (<= 0: the default, 2 s).  The launch then ends by itself with the error
+ * word raised; lbm_synchronize reports LBM_ERR_CUDA and the state is
+ * invalid until new populations are set.  (0, 0) restores the defaults. */
+int lbm_test_barrier_limit(lbm_lattice* h, int32_t missing_arrivals, int64_t timeout_ns);
 
 /* ---- without device allocation ----------------------------------------- */
 /* No counterpart in the reference.  FP64 sums {sum rho, sum m_x, sum m_y,

@@ -338,6 +338,7 @@ typedef struct {
     const uint8_t* flags;      /* (n) cell types, or NULL = all fluid */
     const double* force;       /* (3, n) for FORCE_FIELD */
     const float* porosity;     /* (n) for FORCE_DRAG */
+    double storage_ref_u[3];   /* 16-bit storage reference velocity */
 } orc_lattice;
 
 /* IEEE binary16 / bfloat16 round-to-nearest-even conversions (bit-level). */
@@ -403,29 +404,47 @@ uint16_t orc_f32_to_bf16(float f)
 
 float orc_bf16_to_f32(uint16_t b) { return u2f((uint32_t)b << 16); }
 
-/* Round a population value to what the storage format can hold. */
-static inline double store_round(int storage, int d, double v)
+/* 16-bit storage shift of each direction: (float)(feq_d(1, ref_u) - w_d),
+ * reciprocal form (the GPU's Params::shift_h); zero for the other storages. */
+static void storage_shift(int storage, const double* ref_u, float* sh)
+{
+    const int s16 = storage == STORE_F16_SHIFT || storage == STORE_BF16_SHIFT;
+    const double rx = ref_u ? ref_u[0] : 0.0, ry = ref_u ? ref_u[1] : 0.0, rz = ref_u ? ref_u[2] : 0.0;
+    const double r_sq = rx * rx + ry * ry + rz * rz;
+    for (int d = 0; d < Q; ++d) {
+        double cu = (double)CX[d] * rx + (double)CY[d] * ry + (double)CZ[d] * rz;
+        double feq = W[d] * 1.0 * (1.0 + cu * INV_CS2 + cu * cu * INV_TWO_CS4 - r_sq * INV_TWO_CS2);
+        sh[d] = s16 ? (float)(feq - W[d]) : 0.0f;
+    }
+}
+
+/* Round a population value to what the storage format can hold.  The 16-bit
+ * formats hold the binary16 / bfloat16 rounding of the f32 number
+ * (float)(v - w_d) - sh_d and read back as w_d + ((float)stored + sh_d). */
+static inline double store_round(int storage, float sh, int d, double v)
 {
     switch (storage) {
     case STORE_F32: return (double)(float)v;
     case STORE_F16_SHIFT: {
-        float dev = (float)(v - W[d]);
-        return W[d] + (double)orc_f16_to_f32(orc_f32_to_f16(dev));
+        float dev = (float)(v - W[d]) - sh;
+        return W[d] + (double)(orc_f16_to_f32(orc_f32_to_f16(dev)) + sh);
     }
     case STORE_BF16_SHIFT: {
-        float dev = (float)(v - W[d]);
-        return W[d] + (double)orc_bf16_to_f32(orc_f32_to_bf16(dev));
+        float dev = (float)(v - W[d]) - sh;
+        return W[d] + (double)(orc_bf16_to_f32(orc_f32_to_bf16(dev)) + sh);
     }
     default: return v;
     }
 }
 
-void orc_store_round(int storage, double* f, int64_t n)
+void orc_store_round(int storage, const double* ref_u, double* f, int64_t n)
 {
     init_constants();
+    float sh[Q];
+    storage_shift(storage, ref_u, sh);
 #pragma omp parallel for schedule(static)
     for (int64_t c = 0; c < n; ++c)
-        for (int d = 0; d < Q; ++d) f[d * n + c] = store_round(storage, d, f[d * n + c]);
+        for (int d = 0; d < Q; ++d) f[d * n + c] = store_round(storage, sh[d], d, f[d * n + c]);
 }
 
 static inline int cell_type(const orc_lattice* L, int64_t c)
@@ -433,8 +452,12 @@ static inline int cell_type(const orc_lattice* L, int64_t c)
     return L->flags ? (L->flags[c] & 3) : CELL_FLUID;
 }
 
-/* Value a solid cell holds in storage for direction d: the rest state w_d. */
-static inline double solid_value(const orc_lattice* L, int d) { return store_round(L->storage, d, W[d]); }
+/* The rest state w_d a solid cell stands for, as the arithmetic sees it (f32
+ * storage: w_d in f32; the deviation storages: a zero deviation). */
+static inline double solid_value(const orc_lattice* L, int d)
+{
+    return L->storage == STORE_F32 ? (double)(float)W[d] : W[d];
+}
 
 static void feq_point(double rho, const double* u, double* out)
 {
@@ -584,6 +607,8 @@ static inline void collide_cell(const orc_lattice* L, int64_t c, int64_t n, cons
 void orc_engine_collide_local(const orc_lattice* L, const double* f, double* P, double* rho, double* u)
 {
     init_constants();
+    float sh[Q];
+    storage_shift(L->storage, L->storage_ref_u, sh);
     const int nx = L->nx, ny = L->ny, nz = L->nz;
     const int64_t n = (int64_t)nx * ny * nz;
 #pragma omp parallel for schedule(static)
@@ -597,7 +622,7 @@ void orc_engine_collide_local(const orc_lattice* L, const double* f, double* P, 
             continue;
         }
         collide_cell(L, c, n, fl, o);
-        for (int d = 0; d < Q; ++d) P[d * n + c] = store_round(L->storage, d, o[d]);
+        for (int d = 0; d < Q; ++d) P[d * n + c] = store_round(L->storage, sh[d], d, o[d]);
     }
 }
 
@@ -606,6 +631,8 @@ void orc_engine_collide_local(const orc_lattice* L, const double* f, double* P, 
 void orc_engine_step(const orc_lattice* L, const double* Pin, double* Pout, double* rho, double* u)
 {
     init_constants();
+    float sh[Q];
+    storage_shift(L->storage, L->storage_ref_u, sh);
     const int nx = L->nx, ny = L->ny, nz = L->nz;
     const int64_t n = (int64_t)nx * ny * nz;
 #pragma omp parallel for schedule(static)
@@ -625,7 +652,7 @@ void orc_engine_step(const orc_lattice* L, const double* Pin, double* Pout, doub
                 post_stream_state(L, Pin, gx, y, z, gt, f);
                 if (rho) readback(L, c, n, t, f, rho, u);
                 collide_cell(L, c, n, f, o);
-                for (int d = 0; d < Q; ++d) Pout[d * n + c] = store_round(L->storage, d, o[d]);
+                for (int d = 0; d < Q; ++d) Pout[d * n + c] = store_round(L->storage, sh[d], d, o[d]);
             }
 }
 

@@ -55,6 +55,7 @@ class _OrcLattice(C.Structure):
         ("flags", _u8p),
         ("force", _dp),
         ("porosity", _fp),
+        ("storage_ref_u", C.c_double * 3),
     ]
 
 
@@ -92,7 +93,7 @@ def lib() -> C.CDLL:
         _lib.orc_engine_run.argtypes = [L, _dp, i]
         _lib.orc_engine_run.restype = i
         _lib.orc_conservation.argtypes = [L, _dp, _dp]
-        _lib.orc_store_round.argtypes = [i, _dp, C.c_int64]
+        _lib.orc_store_round.argtypes = [i, _dp, _dp, C.c_int64]
         _lib.orc_constants.argtypes = [_dp, _dp]
         _lib.orc_num_threads.restype = i
         _lib.orc_set_num_threads.argtypes = [i]
@@ -223,10 +224,12 @@ def bf16_bits_to_f32(h: int) -> float:
     return float(lib().orc_bf16_to_f32(int(h)))
 
 
-def store_round(storage: int, f) -> np.ndarray:
+def store_round(storage: int, f, ref_u=(0.0, 0.0, 0.0)) -> np.ndarray:
+    """f rounded to what the storage holds; the 16-bit storages hold the
+    deviation from feq(1, ref_u)."""
     out = _f64(f).copy()
     n = out.size // 19
-    lib().orc_store_round(int(storage), _ptr(out), n)
+    lib().orc_store_round(int(storage), _ptr(_f64(ref_u)), _ptr(out), n)
     return out
 
 
@@ -253,9 +256,13 @@ class OracleLattice:
         drag_k=0.0,
         inflow_rho=1.0,
         inflow_u=(0.0, 0.0, 0.0),
+        storage_ref_u=None,
     ):
         nx, ny, nz = (int(s) for s in shape)
         self.shape = (nx, ny, nz)
+        # the 16-bit storages' reference velocity; default: the inflow
+        # velocity, as the engine's Lattice
+        self.storage_ref_u = tuple(float(v) for v in (inflow_u if storage_ref_u is None else storage_ref_u))
         self.n = nx * ny * nz
         self.storage = int(storage)
         self._flags = None if flags is None else np.ascontiguousarray(flags, dtype=np.uint8)
@@ -275,6 +282,8 @@ class OracleLattice:
             s.inflow_u[k] = float(inflow_u[k])
         s.drag_k = float(drag_k)
         s.inflow_rho = float(inflow_rho)
+        for k in range(3):
+            s.storage_ref_u[k] = self.storage_ref_u[k]
         s.flags = _ptr(self._flags, _u8p)
         s.force = _ptr(self._force)
         s.porosity = _ptr(self._poro, _fp)
@@ -288,7 +297,7 @@ class OracleLattice:
         return C.byref(self._s)
 
     def set_populations(self, f) -> None:
-        self._a = store_round(self.storage, f).reshape((19, *self.shape))
+        self._a = store_round(self.storage, f, self.storage_ref_u).reshape((19, *self.shape))
         self._spare = None
         self._pre = True
 

@@ -1,0 +1,148 @@
+"""The four-cell 16-bit step (k_step4 for the plain quads, k_step4_rules on a
+second stream for the quads that need a boundary rule) on a B200.
+
+Lattices with many solid cells, walled faces, inflow / outflow planes and
+per-cell forces, stepped with the one-, two- and four-cell kernels mixed with
+readback steps, sums steps and the first step after an upload: the three
+give the same bits, and stay within tolerance of the oracle.  Slabs whose
+halo planes cut through spheres stay bit-identical to the unsplit lattice.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+from adjoint_cases import case
+from gpu_cases import pair, random_state
+from helpers import same_bytes
+
+from lattice_boltzmann_d3q19_b200 import Lattice, geometry
+from lattice_boltzmann_d3q19_b200.slab import SlabGroup, slab_bounds
+from test_gpu_slab import gpu_slab
+
+pytestmark = pytest.mark.gpu
+
+FAST_TOL = {"f32": 2e-6, "f16": 2e-4, "bf16": 2e-3}
+
+
+def _scattered_solids(shape, frac, seed):
+    rng = np.random.default_rng(seed)
+    flags = (rng.random(shape) < frac).astype(np.uint8)
+    return flags
+
+
+def _cases(storage):
+    """(name, Lattice kwargs, flags, setup(lat), f0) with nz a multiple of 4."""
+    out = []
+    fl, _ = geometry.sphere_channel((40, 16, 16), n_spheres=5, radius=(2.0, 4.0), seed=7)
+    fl[0] = 2
+    fl[-1] = 3
+    out.append(("channel", dict(shape=(40, 16, 16), tau=0.56, inflow_u=(0.04, 0.0, 0.0)), fl, None,
+                random_state((40, 16, 16), 70, amp=0.01)))
+    out.append(("scattered_solids", dict(shape=(12, 10, 20), tau=0.7), _scattered_solids((12, 10, 20), 0.2, 71),
+                None, random_state((12, 10, 20), 72, amp=0.02)))
+    walls = {"x-": (0.0, 0.01, 0.0), "y+": (0.05, 0.0, 0.0), "z-": (0.0, 0.02, 0.0), "z+": (0.01, 0.0, 0.0)}
+    out.append(("walled_box_solids", dict(shape=(9, 7, 12), tau=0.62, periodic=(False, False, False),
+                                          wall_velocity=walls),
+                _scattered_solids((9, 7, 12), 0.1, 73), None, random_state((9, 7, 12), 74, amp=0.02)))
+    alpha = geometry.smooth_porosity((24, 10, 12), sigma=2.0, seed=9)
+    out.append(("drag", dict(shape=(24, 10, 12), tau=0.7, force_mode="drag", drag_k=0.05,
+                             body_force=(1e-6, 0.0, 0.0), inflow_u=(0.03, 0.0, 0.0)),
+                _scattered_solids((24, 10, 12), 0.05, 75),
+                lambda lat: lat.set_porosity(alpha), random_state((24, 10, 12), 76, amp=0.02)))
+    F = 1e-4 * np.random.default_rng(77).standard_normal((3, 8, 6, 8))
+    out.append(("force_field", dict(shape=(8, 6, 8), tau=0.8, force_mode="field"),
+                _scattered_solids((8, 6, 8), 0.15, 78), lambda lat: lat.set_force_field(F),
+                random_state((8, 6, 8), 79)))
+    return out
+
+
+def _run(kw, flags, setup, f0, storage, cpt, plan):
+    kw = dict(kw)
+    lat = Lattice(kw.pop("shape"), kw.pop("tau"), storage=storage, cells_per_thread=cpt, **kw)
+    with lat:
+        lat.set_flags(flags)
+        if setup:
+            setup(lat)
+        lat.set_populations(f0)
+        frames = []
+        for kind, n in plan:
+            if kind == "step":
+                lat.step(n)
+            elif kind == "capture":
+                _, r, u = lat.run_capture(n, 1)
+                frames.append((r, u))
+            else:
+                frames.append(lat.step_monitor(n))
+        return lat.get_populations(), lat.rho_u(), frames
+
+
+PLAN = [("step", 1), ("step", 7), ("capture", 3), ("step", 4), ("monitor", 3), ("step", 5)]
+
+
+@pytest.mark.parametrize("storage", ["f16", "bf16"])
+def test_four_cell_kernel_matches_two_and_one_cell_kernels(storage):
+    """The four-cell and two-cell kernels share the packed collision: the same
+    bits.  The one-cell kernel's scalar collision rounds differently: within
+    the storage tolerance."""
+    for name, kw, flags, setup, f0 in _cases(storage):
+        outs = {cpt: _run(kw, flags, setup, f0, storage, cpt, PLAN) for cpt in (1, 2, 4)}
+        f_a, (r_a, u_a), fr_a = outs[4]
+        f_b, (r_b, u_b), fr_b = outs[2]
+        assert same_bytes(f_a, f_b), (name, float(np.max(np.abs(f_a - f_b))))
+        assert same_bytes(r_a, r_b) and same_bytes(u_a, u_b), name
+        assert same_bytes(fr_a[0][0], fr_b[0][0]) and same_bytes(fr_a[0][1], fr_b[0][1]), name
+        assert np.array_equal(fr_a[1], fr_b[1]), name  # FP64 monitor sums
+        f_c = outs[1][0]
+        assert float(np.max(np.abs(f_a - f_c))) <= FAST_TOL[storage], name
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
+def test_rule_quads_against_oracle(storage):
+    for name, kw, flags, setup, f0 in _cases(storage):
+        if name in ("drag", "force_field"):
+            continue  # per-cell forces: covered by the kernel-agreement test
+        kw2 = dict(kw)
+        shape, tau = kw2.pop("shape"), kw2.pop("tau")
+        gpu, cpu = pair(shape, tau, storage, flags=flags, **kw2)
+        with gpu:
+            gpu.set_populations(f0)
+            cpu.set_populations(f0)
+            for n in (1, 14):
+                gpu.step(n)
+                cpu.step(n)
+            df = float(np.max(np.abs(gpu.get_populations() - cpu.get_populations())))
+            rg, ug = gpu.rho_u()
+            rc, uc = cpu.rho_u()
+            print(f"{name} {storage}: max|df|={df:.3e}")
+            assert df <= FAST_TOL[storage], (name, df)
+            assert float(np.max(np.abs(ug - uc))) <= 4 * FAST_TOL[storage]
+            assert np.all(rg[flags == 1] == 0.0)
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+def test_slabs_through_spheres_match_unsplit(storage):
+    """Slabs whose halo planes cut through spheres (nz a multiple of 4, so the
+    16-bit slabs run the four-cell kernel): bit-identical to the unsplit
+    lattice."""
+    c = case("drag_channel", shape=(20, 12, 12))
+    assert (c["flags"][[6, 7, 13, 14]] == 1).any()
+    n_steps = 11
+    lat = Lattice(c["shape"], c["tau"], storage=storage, **c["kw"])
+    lat.set_flags(c["flags"])
+    lat.set_porosity(c["alpha"])
+    lat.set_populations(c["f0"])
+    lat.step(n_steps)
+    f_ref = lat.get_populations()
+    lat.close()
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        group = SlabGroup([gpu_slab(c, x0, x1, storage, stream) for x0, x1 in slab_bounds(c["shape"][0], 3)])
+        for s in group.slabs:
+            s.set_populations(c["f0"])
+        group.step(n_steps)
+        f = group.get_populations()
+    for s in group.slabs:
+        s.engine.lat.close()
+    assert np.array_equal(f, f_ref)

@@ -42,14 +42,15 @@ def test_desc_defaults():
 
 
 def test_desc_layout_matches_header():
-    # 6 int32, tau, 18 + 3 doubles, drag_k, inflow_rho, 3 doubles, 4 int32
-    assert C.sizeof(N.LbmDesc) == 6 * 4 + 8 + 21 * 8 + 8 + 8 + 24 + 16
+    # 6 int32, tau, 18 + 3 doubles, drag_k, inflow_rho, 3 doubles, 4 int32,
+    # 3 doubles (storage_ref_u)
+    assert C.sizeof(N.LbmDesc) == 6 * 4 + 8 + 21 * 8 + 8 + 8 + 24 + 16 + 24
 
 
 @pytest.mark.parametrize(
     "field,value",
     [("nx", 0), ("storage", 9), ("force_mode", 7), ("tau", 0.5), ("periodic", 8), ("block_size", 48),
-     ("cells_per_thread", 3), ("staging", 4)],
+     ("cells_per_thread", 3), ("staging", 5)],
 )
 def test_create_rejects_bad_descriptors(field, value):
     d = N.LbmDesc()

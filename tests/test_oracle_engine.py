@@ -175,3 +175,26 @@ def test_bfloat16_conversion(oracle_mod):
         assert O.f32_to_bf16_bits(float(v)) == _bf16_ref(v)
         back = O.bf16_bits_to_f32(O.f32_to_bf16_bits(float(v)))
         assert abs(back - float(v)) <= abs(float(v)) * 2.0**-8
+
+
+def test_store_round_with_reference_velocity(oracle_mod):
+    """The 16-bit storages hold the deviation from feq(1, ref_u): a value v of
+    direction d is stored as the binary16 rounding of the f32 number
+    (float)(v - w_d) - s_d, s_d = (float)(feq_d(1, ref_u) - w_d), and reads
+    back as w_d + ((float)stored + s_d) in f32."""
+    O = oracle_mod
+    ref_u = (0.04, -0.01, 0.005)
+    W = O.constants()[0]
+    feq_ref = O.feq_field(np.ones((1, 1, 1)), np.array(ref_u).reshape(3, 1, 1, 1)).reshape(19)
+    s = (feq_ref - W).astype(np.float32)
+    rng = np.random.default_rng(9)
+    f = feq_ref.reshape(19, 1, 1, 1) * (1.0 + 0.02 * rng.standard_normal((19, 4, 3, 2)))
+    got = O.store_round(O.STORE_F16_SHIFT, f, ref_u)
+    dev = (f - W.reshape(19, 1, 1, 1)).astype(np.float32) - s.reshape(19, 1, 1, 1)
+    back = dev.astype(np.float16).astype(np.float32) + s.reshape(19, 1, 1, 1)
+    assert np.array_equal(got, W.reshape(19, 1, 1, 1) + back.astype(np.float64))
+    # finer than the plain f - w shift for values near the reference state
+    plain = O.store_round(O.STORE_F16_SHIFT, f)
+    assert np.abs(got - f).max() < np.abs(plain - f).max()
+    # zero reference velocity: the plain f - w format
+    assert np.array_equal(O.store_round(O.STORE_F16_SHIFT, f, (0.0, 0.0, 0.0)), plain)
