@@ -880,6 +880,64 @@ def run_slab(args, rank: int, world: int, local_rank: int):
     }), flush=True)
 
 
+def run_moments(args):
+    """The 16-bit moment-encoded state (the reference's frontier format)
+    against FP16-shift storage on the headline sphere channel: per tau an f64
+    run that also calibrates the 19 moment ranges over every post-collision
+    state (margin 5 %), then the moment-encoded run (f32 step kernels, state
+    held as 16-bit moment codes between steps) and the f16 (f - feq(1,
+    u_in)) run, each against the f64 result after the same steps.  Reports
+    the errors and GLUPS (the moment-encoded GLUPS include its decode and
+    encode passes)."""
+    import torch
+
+    from lattice_boltzmann_d3q19_b200 import Lattice
+
+    steps = args.steps
+    flags = channel_geometry()
+    fluid = flags != 1
+    n = int(np.prod(SHAPE))
+    stream = torch.cuda.Stream()
+    rows = []
+    for tau in (0.51, 0.56, 0.8):
+        def lattice(storage):
+            lat = Lattice(SHAPE, tau, storage=storage, inflow_u=(INFLOW_U, 0.0, 0.0))
+            lat.set_stream(stream.cuda_stream)
+            lat.set_flags(flags)
+            lat.set_equilibrium(1.0, (INFLOW_U, 0.0, 0.0))
+            return lat
+
+        ref = lattice("f64")
+        holder = {}
+        t_cal = _device_time(lambda: holder.update(r=ref.moment16_calibrate(steps, 0.05)), torch, stream)
+        lo, hi = holder["r"]
+        _, u64 = ref.rho_u()
+        ref.close()
+        ref_f = u64[:, fluid]
+        umax = np.sqrt((ref_f * ref_f).sum(0)).max()
+        row = {"tau": tau, "calibration_ms": t_cal}
+        for mode in ("moment16", "f16"):
+            lat = lattice("f32" if mode == "moment16" else "f16")
+            if mode == "moment16":
+                ms = _device_time(lambda: lat.moment16_step(lo, hi, steps), torch, stream)
+            else:
+                ms = _device_time(lambda: lat.step(steps), torch, stream)
+            healthy = lat.check_health()
+            _, u = lat.rho_u()
+            lat.close()
+            du = (u - u64)[:, fluid]
+            row[mode] = {"glups": n * steps / (ms / 1e3) / 1e9, "healthy": healthy,
+                         "u_err_l2_rel": float(np.linalg.norm(du) / np.linalg.norm(ref_f)),
+                         "u_err_max_rel": float(np.sqrt((du * du).sum(0)).max() / umax)}
+        rows.append(row)
+    print(json.dumps({"metric": "16-bit moment-encoded state vs FP16-shift storage", "workload": "moments",
+                      "unit": "GLUPS", "value": statistics.median(r["moment16"]["glups"] for r in rows),
+                      "steps": steps, "results": rows,
+                      "config": {"workload": WORKLOAD, "ranges": "f64 envelope over the run, margin 5 %",
+                                 "moment16_bytes_per_cell": "decode 38 + 76, step 153, encode 76 + 38"}}),
+          flush=True)
+
+
 ADJ_STEPS, ADJ_EVERY = 2000, 50
 
 
@@ -1013,7 +1071,8 @@ def main():
     ap.add_argument("--repeats", type=int, default=REPEATS)
     ap.add_argument("--cells-per-thread", type=int, default=0, choices=[0, 1, 2, 4])
     ap.add_argument("--staging", default="auto", choices=["auto", "registers", "tma", "pipelined", "persistent"])
-    ap.add_argument("--workload", default="channel", choices=["channel", "cavity", "sweep", "ensemble", "adjoint", "slab"])
+    ap.add_argument("--workload", default="channel",
+                    choices=["channel", "cavity", "sweep", "ensemble", "adjoint", "slab", "moments"])
     args = ap.parse_args()
     global CELLS_PER_THREAD, STAGING
     CELLS_PER_THREAD = args.cells_per_thread
@@ -1030,8 +1089,8 @@ def main():
         run_slab(args, rank, world, local_rank)
         return
     if args.workload != "channel":
-        {"cavity": run_cavity, "sweep": run_sweep, "ensemble": run_ensemble,
-         "adjoint": run_adjoint}[args.workload](args)
+        {"cavity": run_cavity, "sweep": run_sweep, "ensemble": run_ensemble, "adjoint": run_adjoint,
+         "moments": run_moments}[args.workload](args)
         return
     run_ours(args, rank, world, local_rank)
 

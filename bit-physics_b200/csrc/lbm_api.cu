@@ -185,7 +185,7 @@ cudaError_t lbm::api::launch(lbm_lattice* h, int kernel, const void* src, void* 
     a.pipe_grid = kernel == KERNEL_STEP ? h->pipe_grid : 0;
     a.sums_grid = kernel == KERNEL_STEP ? h->sums_grid : 0;
     a.rule_quads = h->rule_quads;
-    a.rule_count = h->rule_count;
+    for (int k = 0; k < QUAD_KINDS; ++k) a.rule_counts[k] = h->rule_counts[k];
     a.side = h->side;
     a.fork = h->ev_fork;
     a.join = h->ev_join;
@@ -205,9 +205,11 @@ namespace {
 int refresh_rule_quads(lbm_lattice* h)
 {
     if (h->vec != 4) return LBM_OK;
-    int* count = h->rule_quads + h->n / 4;
-    CK(launch_list_rule_quads(h->P, h->rule_quads, count, h->stream), "rule quad list");
-    CK(cudaMemcpyAsync(&h->rule_count, count, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "rule quad count");
+    const int cap = h->n / 4;
+    int* counts = h->rule_quads + (size_t)QUAD_KINDS * cap;
+    CK(launch_list_rule_quads(h->P, h->rule_quads, cap, counts, h->stream), "rule quad lists");
+    CK(cudaMemcpyAsync(h->rule_counts, counts, sizeof(int) * QUAD_KINDS, cudaMemcpyDeviceToHost, h->stream),
+       "rule quad counts");
     CK(cudaStreamSynchronize(h->stream), "rule quad sync");
     h->params_version += 1;  // a captured step graph holds the old count
     return LBM_OK;
@@ -461,7 +463,7 @@ int lbm_create(const lbm_desc* desc, lbm_lattice** out)
         h->persist = true;
     }
     if (h->vec == 4) {
-        e = cudaMalloc((void**)&h->rule_quads, sizeof(int) * ((size_t)h->n / 4 + 1));
+        e = cudaMalloc((void**)&h->rule_quads, sizeof(int) * ((size_t)QUAD_KINDS * (h->n / 4) + QUAD_KINDS));
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming);
@@ -487,7 +489,8 @@ int lbm_destroy(lbm_lattice* h)
     if (h->graph) cudaGraphExecDestroy(h->graph);
     if (h->side) cudaStreamSynchronize(h->side);
     void* ptrs[] = {h->buf[0], h->buf[1], h->flags, h->bbmask, h->force, h->poro, h->rho,
-                    h->u, h->partials, h->sums, h->staging, h->monitor, h->err, h->diag, h->rule_quads, h->bar};
+                    h->u, h->partials, h->sums, h->staging, h->monitor, h->err, h->diag, h->rule_quads, h->bar,
+                    h->me_codes};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);

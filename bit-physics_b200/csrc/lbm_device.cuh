@@ -730,28 +730,40 @@ __device__ __forceinline__ void gather(const Params& P, const Streams<typename M
     for (int d = 0; d < Q; ++d) f[d] = M::load(P, S.src[d] + nb.src(d), d);
 }
 
-// Replace the pulled values that a boundary rule overrides.  Replacement
-// values are re-loaded from memory (never read from f[], which may already
-// hold replaced entries), so every rule sees the raw gather as the reference
-// does (bgk.py:190-216 reads its input f and writes a copy).
+// Replace the pulled values that a boundary rule overrides; every rule sees
+// the raw gather as the reference does (bgk.py:190-216 reads its input f and
+// writes a copy).
 //   walled face crossed:  f[d] = raw[opp(d)] + injection(face, rho_w)
 //   solid source (mask):  f[d] = P[opp(d)] at the cell (half-way bounce-back)
+// A face rule reads only the raw value of the opposite direction, so each
+// opposite pair (d, opp(d)) is resolved from its two raw values held in
+// registers (both taken before either is replaced: at an edge or corner both
+// members of a pair can cross a face).  The bounce-back values are loads of
+// the cell's own slots; their directions cross no face.
 template <class M, class F>
 __device__ __forceinline__ void boundary_fix(const Params& P, const Streams<typename M::T>& S, const Nbr& nb,
                                              int gx, int y, int z, int gidx, bool face_cell, uint32_t bbmask,
                                              F&& f)
 {
     using C = typename M::C;
-    C rho_w = C(0);
-    if (face_cell) rho_w = M::rho_wall(P, f);
+    if (face_cell) {
+        const C rho_w = M::rho_wall(P, f);
 #pragma unroll
-    for (int d = 1; d < Q; ++d) {
-        const int face = face_cell ? crossed_face(P, d, gx, y, z) : -1;
-        const int o = opp(d);
-        if (face >= 0) {
-            f[d] = M::load(P, S.src[o] + nb.src(o), o) + M::inject(P, face, d, rho_w);
-        } else if ((bbmask >> d) & 1u) {
-            f[d] = M::load(P, S.src[o] + gidx, o);
+        for (int d = 1; d < Q; d += 2) {
+            const int o = d + 1;
+            const int fd = crossed_face(P, d, gx, y, z), fo = crossed_face(P, o, gx, y, z);
+            const C rd = f[d], ro = f[o];
+            if (fd >= 0) f[d] = ro + M::inject(P, fd, d, rho_w);
+            if (fo >= 0) f[o] = rd + M::inject(P, fo, o, rho_w);
+            if (fd >= 0) bbmask &= ~(1u << d);
+            if (fo >= 0) bbmask &= ~(1u << o);
+        }
+    }
+    if (bbmask) {
+#pragma unroll
+        for (int d = 1; d < Q; ++d) {
+            const int o = opp(d);
+            if ((bbmask >> d) & 1u) f[d] = M::load(P, S.src[o] + gidx, o);
         }
     }
 }

@@ -6,7 +6,7 @@
 
 namespace lbm {
 
-__global__ void k_list_rule_quads(Params P, int* __restrict__ list, int* __restrict__ count)
+__global__ void k_list_rule_quads(Params P, int* __restrict__ lists, int cap, int* __restrict__ counts)
 {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     const int idx0 = 4 * q;
@@ -14,14 +14,29 @@ __global__ void k_list_rule_quads(Params P, int* __restrict__ list, int* __restr
     int x, y, z0;
     decode_xyz(P, idx0, x, y, z0);
     const uint32_t fl4 = P.has_flags ? *reinterpret_cast<const uint32_t*>(P.flags + idx0) : 0u;
-    if (fl4 != 0u || quad_on_walled_face(P, x, y, z0)) list[atomicAdd(count, 1)] = q;
+    const bool face = quad_on_walled_face(P, x, y, z0);
+    if (!face && (fl4 == 0u || fl4 == QUAD_SOLID || fl4 == QUAD_INFLOW)) return;  // k_step4 steps it
+    int kind = QUAD_KIND_OTHER;
+    if (!face) {
+        // bytes of four cells, each fluid or solid (near-solid bits allowed)
+        const uint32_t t = fl4 & 0x03030303u;
+        const bool fluid_or_solid = ((t & 0x02020202u) == 0u);
+        if (fluid_or_solid) {
+            kind = QUAD_KIND_NEAR;
+        } else if (fl4 == QUAD_OUTFLOW) {
+            const int gx = x == 0 ? P.nx - 1 : x - 1;
+            const uint32_t g4 = *reinterpret_cast<const uint32_t*>(P.flags + idx0 + (gx - x) * P.nynz);
+            if (g4 == 0u && !quad_on_walled_face(P, gx, y, z0)) kind = QUAD_KIND_OUTFLOW;
+        }
+    }
+    lists[(size_t)kind * cap + atomicAdd(counts + kind, 1)] = q;
 }
 
-cudaError_t launch_list_rule_quads(const Params& P, int* list, int* count, cudaStream_t s)
+cudaError_t launch_list_rule_quads(const Params& P, int* lists, int cap, int* counts, cudaStream_t s)
 {
-    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(int), s);
+    cudaError_t e = cudaMemsetAsync(counts, 0, sizeof(int) * QUAD_KINDS, s);
     if (e != cudaSuccess) return e;
-    k_list_rule_quads<<<grid_for(P.n / 4, 256), 256, 0, s>>>(P, list, count);
+    k_list_rule_quads<<<grid_for(P.n / 4, 256), 256, 0, s>>>(P, lists, cap, counts);
     return cudaGetLastError();
 }
 
@@ -32,18 +47,23 @@ template <class M, int FM>
 static cudaError_t launch_step4(const LaunchArgs& a, const Streams<typename M::T>& S)
 {
     cudaError_t e = cudaSuccess;
-    if (a.rule_count > 0) {
+    const int total = a.rule_counts[0] + a.rule_counts[1] + a.rule_counts[2];
+    if (total > 0) {
         if ((e = cudaEventRecord(a.fork, a.stream)) != cudaSuccess) return e;
         if ((e = cudaStreamWaitEvent(a.side, a.fork, 0)) != cudaSuccess) return e;
-        k_step4_rules<M, FM><<<grid_for(2LL * a.rule_count, 128), 128, 0, a.side>>>(a.P, S, a.rule_quads,
-                                                                                   a.rule_count);
+        const int* L = a.rule_quads;
+        const size_t cap = (size_t)a.P.n / 4;
+        const int rgrid = a.rules_grid > 0 ? a.rules_grid : grid_for(2LL * total, 128);
+        k_step4_rules<M, FM><<<rgrid, 128, 0, a.side>>>(
+            a.P, S, L + QUAD_KIND_NEAR * cap, L + QUAD_KIND_OUTFLOW * cap, L + QUAD_KIND_OTHER * cap,
+            a.rule_counts[QUAD_KIND_NEAR], a.rule_counts[QUAD_KIND_OUTFLOW], a.rule_counts[QUAD_KIND_OTHER]);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         if ((e = cudaEventRecord(a.join, a.side)) != cudaSuccess) return e;
     }
     const int block = a.block < 128 ? a.block : 128;  // the kernel's bound
     k_step4<M, FM><<<grid_for(a.P.n / 4, block), block, 0, a.stream>>>(a.P, S);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if (a.rule_count > 0) e = cudaStreamWaitEvent(a.stream, a.join, 0);
+    if (total > 0) e = cudaStreamWaitEvent(a.stream, a.join, 0);
     return e;
 }
 

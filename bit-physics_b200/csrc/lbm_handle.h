@@ -32,6 +32,7 @@ struct lbm_lattice {
     double* staging = nullptr; // (19, n) f64, allocated on first use
     double* monitor = nullptr; // (monitor_cap, 5) per-step sums of lbm_step_monitor
     double* diag = nullptr;    // DIAG_SCRATCH + 6 doubles of lbm_diagnostics, allocated on first use
+    uint16_t* me_codes = nullptr; // (19, n) 16-bit moment codes of lbm_moment16_step, allocated on first use
     int monitor_cap = 0;
     int64_t steps = 0;
     int block = 256;
@@ -49,8 +50,8 @@ struct lbm_lattice {
     int sums_grid = 0;  // > 0: steps with FP64 sums run k_step2_sums
     // Four-cell steps (vec == 4): the quads that need a boundary rule, stepped
     // by k_step4_rules on a second stream beside k_step4.
-    int* rule_quads = nullptr;  // (n / 4 + 1): the list, then its length
-    int rule_count = 0;
+    int* rule_quads = nullptr;  // QUAD_KINDS lists of n / 4 entries, then the counts
+    int rule_counts[lbm::QUAD_KINDS] = {0, 0, 0};
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     // Many steps per cooperative launch (LBM_STAGING_PERSISTENT): barrier

@@ -576,6 +576,20 @@ __device__ __forceinline__ uint32_t pack_dev2(float a, float b, __nv_bfloat16)
 // A quad -- four z-adjacent cells z0..z0 + 3 of one row, z0 a multiple of 4
 // -- is plain when its four cells are fluid, none pulls from a solid cell
 // and none lies on a walled face: its post-stream state is the raw gather.
+// k_step4 also steps the quads of four solid cells (the rest state) and of
+// four inflow cells (feq(inflow) in every cell) off the walled faces; the
+// other quads are rule quads, listed by kind for k_step4_rules:
+//   QUAD_KIND_NEAR     fluid and solid cells only, off the walled faces: one
+//                      round of loads (gather, cell words and the pair's own
+//                      slots, the half-way bounce-back sources) per pair;
+//   QUAD_KIND_OUTFLOW  four outflow cells off the walled faces whose x - 1
+//                      neighbours are plain fluid cells: the plain gather at
+//                      x - 1 (zero gradient);
+//   QUAD_KIND_OTHER    everything else, through the general two-cell step.
+constexpr uint32_t QUAD_SOLID = 0x01010101u;   // flag bytes of four solid cells
+constexpr uint32_t QUAD_INFLOW = 0x02020202u;
+constexpr uint32_t QUAD_OUTFLOW = 0x03030303u;
+enum QuadKind : int { QUAD_KIND_NEAR = 0, QUAD_KIND_OUTFLOW = 1, QUAD_KIND_OTHER = 2, QUAD_KINDS = 3 };
 __device__ __forceinline__ bool quad_on_walled_face(const Params& P, int x, int y, int z0)
 {
     return on_walled_face(P, x, y, z0) || on_walled_face(P, x, y, z0 + 3);
@@ -617,7 +631,20 @@ __global__ void __launch_bounds__(128, 4) k_step4(Params P, Streams<typename M::
         edge[d] = cz(d) == 1 ? (uint32_t)__ldg(p + nb0.Z[0]) : (cz(d) == -1 ? (uint32_t)__ldg(p + zr) : 0u);
     }
     const uint32_t fl4 = P.has_flags ? __ldg(reinterpret_cast<const uint32_t*>(P.flags + idx0)) : 0u;
-    if (fl4 != 0u || quad_on_walled_face(P, x, y, z0)) return;  // a rule quad: k_step4_rules
+    if (fl4 != 0u || quad_on_walled_face(P, x, y, z0)) {
+        if (fl4 != QUAD_SOLID && fl4 != QUAD_INFLOW) return;  // a rule quad: k_step4_rules
+        if (quad_on_walled_face(P, x, y, z0)) return;
+        if (fl4 == QUAD_SOLID) {  // four solid cells: the rest state
+#pragma unroll
+            for (int d = 0; d < Q; ++d) {
+                const float2 sv = M::shift2(P, d, make_float2(0.0f, 0.0f));
+                const uint32_t w = pack_dev2(sv.x, sv.y, T{});
+                *reinterpret_cast<uint2*>(S.dst[d] + idx0) = make_uint2(w, w);
+            }
+            return;
+        }
+    }
+    const bool inflow4 = fl4 == QUAD_INFLOW;  // four inflow cells: feq(inflow) in every cell
     uint32_t lo[Q];  // stored words of cells z0, z0 + 1
 #pragma unroll
     for (int half = 0; half < 2; ++half) {
@@ -628,7 +655,7 @@ __global__ void __launch_bounds__(128, 4) k_step4(Params P, Streams<typename M::
             if (cz(d) == 0) w = half == 0 ? raw[d].x : raw[d].y;
             else if (cz(d) == 1) w = half == 0 ? (raw[d].x << 16) | edge[d] : __funnelshift_r(raw[d].x, raw[d].y, 16);
             else w = half == 0 ? __funnelshift_r(raw[d].x, raw[d].y, 16) : __funnelshift_r(raw[d].y, edge[d], 16);
-            h[d] = M::unshift2(P, d, word_dev2(w, T{}));
+            h[d] = inflow4 ? make_float2(P.inflow_h[d], P.inflow_h[d]) : M::unshift2(P, d, word_dev2(w, T{}));
         }
         M::template collide2<FM>(P, idx0 + 2 * half, h, [&](int d, float2 v) {
             const float2 sv = M::shift2(P, d, v);
@@ -639,22 +666,76 @@ __global__ void __launch_bounds__(128, 4) k_step4(Params P, Streams<typename M::
     }
 }
 
-// The quads of k_step4 that need a boundary rule (quads[0..count) of the
-// lattice's list, launch_list_rule_quads), one pair per thread through the
-// two-cell step.
+// One rule-quad pair task of k_step4_rules: tasks [0, 2 n_near) take the
+// NEAR list, then the OUTFLOW list, then the OTHER list.
 template <class M, int FM>
-__global__ void __launch_bounds__(128) k_step4_rules(Params P, Streams<typename M::T> S,
-                                                     const int* __restrict__ quads, int count)
+__device__ __forceinline__ void rule_pair(const Params& P, const Streams<typename M::T>& S, const int* near_q,
+                                          const int* out_q, const int* other_q, int n_near, int n_out, int n_other,
+                                          int k)
 {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= 2 * count) return;
+    using T = typename M::T;
+    if (k < 2 * n_near) {
+        const int idx0 = 4 * near_q[k >> 1] + 2 * (k & 1);
+        int x, y, z0;
+        decode_xyz(P, idx0, x, y, z0);
+        const Nbr nb0 = make_nbr(P, x, y, z0);
+        const int zp1 = z0 + 2 == P.nz ? 0 : z0 + 2;
+        float2 h[Q];
+        gather_pair<M>(P, S, nb0, z0, zp1, h);
+        const uint2 cw = __ldg(reinterpret_cast<const uint2*>(P.bbmask + idx0));
+        // the pair's own slots: half-way bounce-back sources, loaded with the gather
+        uint32_t own[Q];
+#pragma unroll
+        for (int d = 1; d < Q; ++d) own[d] = __ldg(reinterpret_cast<const unsigned int*>(S.src[d] + idx0));
+        const bool fluid0 = ((cw.x >> CW_FLAG_SHIFT) & 3) == CELL_FLUID;
+        const bool fluid1 = ((cw.y >> CW_FLAG_SHIFT) & 3) == CELL_FLUID;
+        const uint32_t m0 = fluid0 ? cw.x & CW_MASK_BITS : 0u, m1 = fluid1 ? cw.y & CW_MASK_BITS : 0u;
+#pragma unroll
+        for (int d = 1; d < Q; ++d) {
+            const float2 b = M::unshift2(P, opp(d), word_dev2(own[opp(d)], T{}));
+            if ((m0 >> d) & 1u) h[d].x = b.x;
+            if ((m1 >> d) & 1u) h[d].y = b.y;
+        }
+        M::template collide2<FM>(P, idx0, h, [&](int d, float2 v) { store_pair<M>(P, S, idx0, d, v, fluid0, fluid1); });
+        return;
+    }
+    k -= 2 * n_near;
+    if (k < 2 * n_out) {
+        const int idx0 = 4 * out_q[k >> 1] + 2 * (k & 1);
+        int x, y, z0;
+        decode_xyz(P, idx0, x, y, z0);
+        const int gx = x == 0 ? P.nx - 1 : x - 1;
+        const int zp1 = z0 + 2 == P.nz ? 0 : z0 + 2;
+        float2 h[Q];
+        gather_pair<M>(P, S, make_nbr(P, gx, y, z0), z0, zp1, h);
+        M::template collide2<FM>(P, idx0, h, [&](int d, float2 v) { store_pair<M>(P, S, idx0, d, v, true, true); });
+        return;
+    }
+    k -= 2 * n_out;
+    if (k >= 2 * n_other) return;
     const Outputs<float> none{nullptr, nullptr, nullptr};
-    step_pair<M, FM, OUT_NONE>(P, S, none, 4 * quads[k >> 1] + 2 * (k & 1), nullptr);
+    step_pair<M, FM, OUT_NONE>(P, S, none, 4 * other_q[k >> 1] + 2 * (k & 1), nullptr);
 }
 
-// List of the quads that are not plain (order unspecified; each quad's work
-// is independent of the others'); *count on the device.
-__global__ void k_list_rule_quads(Params P, int* __restrict__ list, int* __restrict__ count);
+// The rule quads of k_step4 in a grid-stride loop over the pair tasks.  The
+// launch gives it a small grid: it runs beside k_step4 on a few SMs, its
+// latency-bound tasks spread over k_step4's run, instead of filling every SM
+// for a short while and holding k_step4's blocks back.
+template <class M, int FM>
+__global__ void __launch_bounds__(128) k_step4_rules(Params P, Streams<typename M::T> S, const int* __restrict__ near_q,
+                                                     const int* __restrict__ out_q, const int* __restrict__ other_q,
+                                                     int n_near, int n_out, int n_other)
+{
+    const int total = 2 * (n_near + n_out + n_other);
+#pragma unroll 1
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x)
+        rule_pair<M, FM>(P, S, near_q, out_q, other_q, n_near, n_out, n_other, k);
+}
+
+// Lists of the rule quads by kind: quad indices of kind k at lists + k * cap,
+// their number in counts[k] (order unspecified; each quad's work is
+// independent of the others').
+__global__ void k_list_rule_quads(Params P, int* __restrict__ lists, int cap, int* __restrict__ counts);
 
 // ---------------------------------------------------------------------------
 // Many steps in one cooperative launch (lattices that fit in L2)

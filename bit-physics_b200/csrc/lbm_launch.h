@@ -39,8 +39,9 @@ struct LaunchArgs {
                         // k_step2_sums with this grid
     // vec == 4 steps without outputs: the rule quads (k_step4_rules) run on
     // `side` between the fork and join events
-    const int* rule_quads = nullptr;
-    int rule_count = 0;
+    const int* rule_quads = nullptr;  // QUAD_KINDS lists of n / 4 entries
+    int rule_counts[QUAD_KINDS] = {0, 0, 0};
+    int rules_grid = 0;  // blocks of k_step4_rules (0: one task per thread)
     cudaStream_t side = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
 };
@@ -66,8 +67,9 @@ cudaError_t launch_feq_init(int storage, const Params& P, const double* rho, con
                             cudaStream_t s);
 cudaError_t launch_mark_near_solid(const Params& P, uint8_t* flags, uint32_t* bbmask, cudaStream_t s);
 // The quads of a lattice (nz a multiple of 4) that k_step4 leaves to
-// k_step4_rules, into list; their number into *count (device).
-cudaError_t launch_list_rule_quads(const Params& P, int* list, int* count, cudaStream_t s);
+// k_step4_rules, by kind into lists + kind * cap; their numbers into
+// counts[QUAD_KINDS] (device).
+cudaError_t launch_list_rule_quads(const Params& P, int* lists, int cap, int* counts, cudaStream_t s);
 cudaError_t launch_reduce_partials(const double* partials, int nblocks, double* out5, cudaStream_t s);
 // Tier-1 / Tier-2 diagnostics of f64 rho (n) / u (3, n) device arrays into
 // out6 (device): {check_health, rho_min, rho_max, u_max_lat,

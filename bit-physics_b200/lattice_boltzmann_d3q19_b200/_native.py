@@ -121,6 +121,9 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "lbm_get_rho_u_dev": ([_h, _h, _h], C.c_int),
     "lbm_diagnostics": ([_h, C.c_double, _dp], C.c_int),
     "lbm_test_barrier_limit": ([_h, C.c_int32, C.c_int64], C.c_int),
+    "lbm_moment16_basis": ([_dp, _dp], C.c_int),
+    "lbm_moment16_calibrate": ([_h, C.c_int32, C.c_double, _dp, _dp], C.c_int),
+    "lbm_moment16_step": ([_h, _dp, _dp, C.c_int32], C.c_int),
     "lbm_set_porosity_dev": ([_h, _h], C.c_int),
     "lbm_tape_forward": ([_h, _i, _i, C.POINTER(_h)], C.c_int),
     "lbm_tape_backward": ([_h, _h, _h, _h, _h], C.c_int),

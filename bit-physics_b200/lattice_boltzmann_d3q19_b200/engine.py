@@ -259,6 +259,19 @@ class Lattice:
         keys = ("check_health", "rho_min", "rho_max", "u_max_lat", "check_divergence_free", "check_circulation")
         return {k: float(v) for k, v in zip(keys, out, strict=True)}
 
+    # -- 16-bit moment-encoded state (the reference's frontier format) --------
+    def moment16_calibrate(self, n_steps: int, margin: float = 0.05) -> tuple[np.ndarray, np.ndarray]:
+        """Step n_steps and return the (lo, hi) ranges of the 19 moments over
+        every post-collision state of the run, widened by margin * span."""
+        lo, hi = np.empty(19), np.empty(19)
+        N.check(N.lib().lbm_moment16_calibrate(self._h, int(n_steps), float(margin), N.ptr(lo), N.ptr(hi)))
+        return lo, hi
+
+    def moment16_step(self, lo, hi, n_steps: int) -> None:
+        """Advance n_steps (f32 lattice) with the state between steps held as
+        16-bit moment codes over the ranges [lo, hi]."""
+        N.check(N.lib().lbm_moment16_step(self._h, N.ptr(N.f64(lo)), N.ptr(N.f64(hi)), int(n_steps)))
+
     def check_health(self) -> bool:
         rc = N.lib().lbm_check_health(self._h)
         if rc == N.LBM_ERR_NONFINITE:

@@ -299,6 +299,24 @@ int lbm_tape_destroy(lbm_tape* t);
  * circulation sum's order of summation. */
 int lbm_diagnostics(lbm_lattice* h, double dx_phys, double* out6);
 
+/* ---- 16-bit moment-encoded state ---------------------------------------
+ * The frontier variant's compressed state (packages/lattice-boltzmann-d3q19-
+ * frontier-moment-encoded/src/lbm_me.cpp:71-138, :212-250): 19 monomial
+ * moments per cell (m = M f) quantised to 16 bits over per-moment ranges
+ * [lo_k, hi_k], code = round((m - lo) / (hi - lo) * 65535) clamped.
+ * lbm_moment16_basis: M and M^-1 (19 x 19, row-major; either may be NULL).
+ * lbm_moment16_calibrate: run n_steps on h (f64 or f32 storage) and return
+ * the envelope of every post-collision state's moments over the non-solid
+ * cells, each range widened by margin * its span on both sides.
+ * lbm_moment16_step: advance an f32 lattice n_steps with the persistent
+ * state held as moment codes: each step decodes the codes, runs the fused
+ * step and encodes its result; afterwards the lattice holds the decoded
+ * codes (readbacks and later steps see the encoded state).  No counterpart
+ * in the reference's Stack-E API. */
+int lbm_moment16_basis(double* m_out, double* minv_out);
+int lbm_moment16_calibrate(lbm_lattice* h, int32_t n_steps, double margin, double* lo, double* hi);
+int lbm_moment16_step(lbm_lattice* h, const double* lo, const double* hi, int32_t n_steps);
+
 /* Test hook of the persistent step's bounded grid barrier: the next
  * cooperative launches of h expect `missing_arrivals` more blocks than they
  * launch (so no barrier opens) and give up each wait after timeout_ns
