@@ -810,27 +810,23 @@ def run_ensemble(args):
                       / out["per_lattice_launches"]["glups"]}), flush=True)
 
 
-def run_slab(args, rank: int, world: int, local_rank: int):
-    """x-slab strong scaling: the headline sphere channel (256 x 128 x 128)
-    split in x over the ranks, one slab per GPU with a halo plane per side;
-    every step exchanges 5 populations per face with its neighbours (NCCL
-    point-to-point; one rank exchanges with itself).  Value: global cells x
-    steps / (max over ranks of the CUDA-event time)."""
+def slab_leg(args, rank: int, world: int, local_rank: int, storage: str, overlap: bool):
+    """Time args.steps steps of this rank's x-slab of the headline channel
+    (after args.warmup steps): whole-slab steps after a blocking exchange, or
+    the overlapped step (interior planes while the faces travel on a second
+    stream).  Returns (max over ranks of the CUDA-event ms, healthy, planes
+    of this slab).  With world > 1 the process group must be up."""
     import torch
 
     from lattice_boltzmann_d3q19_b200 import Lattice
     from lattice_boltzmann_d3q19_b200.slab import GpuEngine, SlabLattice, exchange_distributed, slab_bounds, \
-        with_halos
+        step_distributed, with_halos
 
-    dist_on = world > 1
-    if dist_on:
-        torch.distributed.init_process_group("nccl", timeout=timedelta(seconds=300))
-    torch.cuda.set_device(local_rank)
-    storage = args.storage
     nx = SHAPE[0]
     flags = channel_geometry()
     x0, x1 = slab_bounds(nx, world)[rank]
     stream = torch.cuda.Stream()
+    comm = torch.cuda.Stream()
     with torch.cuda.stream(stream):
         lat = Lattice((x1 - x0 + 2, *SHAPE[1:]), TAU, storage=storage, inflow_u=(INFLOW_U, 0.0, 0.0),
                       device=local_rank)
@@ -841,6 +837,9 @@ def run_slab(args, rank: int, world: int, local_rank: int):
 
         def advance(k):
             for _ in range(k):
+                if overlap:
+                    step_distributed(slab, rank, world, comm)
+                    continue
                 if slab.stepped:
                     exchange_distributed(slab, rank, world)
                 lat.step(1)
@@ -849,34 +848,56 @@ def run_slab(args, rank: int, world: int, local_rank: int):
         advance(args.warmup)
         start = torch.cuda.Event(enable_timing=True)
         end = torch.cuda.Event(enable_timing=True)
-        if dist_on:
+        if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
         start.record(stream)
         advance(args.steps)
         end.record(stream)
         torch.cuda.synchronize()
-        if dist_on:
+        if world > 1:
             torch.distributed.barrier()
         ms = start.elapsed_time(end)
         healthy = lat.check_health()
         lat.close()
-    ms_max = ms
-    if dist_on:
+    if world > 1:
         t = torch.tensor([ms], device=f"cuda:{local_rank}", dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_max = float(t.item())
+        ms = float(t.item())
+    return ms, healthy, x1 - x0
+
+
+def run_slab(args, rank: int, world: int, local_rank: int):
+    """x-slab strong scaling: the headline sphere channel (256 x 128 x 128)
+    split in x over the ranks, one slab per GPU with a halo plane per side;
+    every step exchanges 5 populations per face with its neighbours (NCCL
+    point-to-point; one rank exchanges with itself).  Both step forms are
+    timed; value: the overlapped one, global cells x steps / (max over ranks
+    of the CUDA-event time)."""
+    import torch
+
+    dist_on = world > 1
+    if dist_on:
+        torch.distributed.init_process_group("nccl", timeout=timedelta(seconds=300))
+    torch.cuda.set_device(local_rank)
+    storage = args.storage
+    n = int(np.prod(SHAPE))
+    legs = {}
+    for name, overlap in (("whole_slab", False), ("overlapped", True)):
+        ms, healthy, planes = slab_leg(args, rank, world, local_rank, storage, overlap)
+        legs[name] = {"glups": n * args.steps / (ms / 1e3) / 1e9, "ms_per_step": ms / args.steps, "healthy": healthy}
+    if dist_on:
         torch.distributed.destroy_process_group()
     if rank != 0:
         return
-    n = int(np.prod(SHAPE))
     elem = {"f64": 8, "f32": 4, "f16": 2, "bf16": 2}[storage]
     print(json.dumps({
         "metric": "D3Q19 GLUPS, x-slab decomposition of one lattice", "workload": "slab", "unit": "GLUPS",
-        "value": n * args.steps / (ms_max / 1e3) / 1e9, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "scaling": "strong", "dtype": storage,
-        "healthy": healthy, "halo_bytes_per_face_per_step": 5 * SHAPE[1] * SHAPE[2] * elem,
-        "config": {"workload": WORKLOAD, "slabs": world, "planes_per_slab": x1 - x0},
+        "value": legs["overlapped"]["glups"], "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": legs["overlapped"]["ms_per_step"], "scaling": "strong",
+        "dtype": storage, "variants": legs, "healthy": all(v["healthy"] for v in legs.values()),
+        "halo_bytes_per_face_per_step": 5 * SHAPE[1] * SHAPE[2] * elem,
+        "config": {"workload": WORKLOAD, "slabs": world, "planes_per_slab": planes},
     }), flush=True)
 
 

@@ -215,6 +215,14 @@ int refresh_rule_quads(lbm_lattice* h)
     return LBM_OK;
 }
 
+// Calls that change the state or the parameters wait for an open
+// plane-range step to be committed.
+int check_no_open_step(const lbm_lattice* h)
+{
+    if (h->open_step) return fail(LBM_ERR_STATE, "a plane-range step is open (lbm_step_commit ends it)");
+    return LBM_OK;
+}
+
 int ensure_staging(lbm_lattice* h)
 {
     if (h->staging) return LBM_OK;
@@ -505,6 +513,7 @@ int lbm_set_stream(lbm_lattice* h, void* stream)
 {
     int rc = check_handle(h);
     if (rc) return rc;
+    if ((rc = check_no_open_step(h))) return rc;
     CK(cudaStreamSynchronize(h->stream), "stream sync");
     if (h->own_stream) CK(cudaStreamDestroy(h->stream), "stream destroy");
     h->own_stream = false;
@@ -543,6 +552,7 @@ int lbm_set_populations(lbm_lattice* h, const double* f)
 {
     int rc = check_handle(h);
     if (rc) return rc;
+    if ((rc = check_no_open_step(h))) return rc;
     if (!f) return fail(LBM_ERR_INVALID, "null population array");
     const size_t bytes = sizeof(double) * Q * (size_t)h->n;
     if (h->storage == LBM_STORAGE_F64) {
@@ -583,6 +593,7 @@ int lbm_set_equilibrium(lbm_lattice* h, const double* rho, const double* u)
 {
     int rc = check_handle(h);
     if (rc) return rc;
+    if ((rc = check_no_open_step(h))) return rc;
     double* drho = nullptr;
     double* du = nullptr;
     const size_t n = (size_t)h->n;
@@ -603,6 +614,7 @@ int lbm_set_flags(lbm_lattice* h, const uint8_t* flags)
 {
     int rc = check_handle(h);
     if (rc) return rc;
+    if ((rc = check_no_open_step(h))) return rc;
     if (!flags) {
         h->has_flags = false;
         rebuild_params(h);
@@ -637,6 +649,7 @@ int lbm_set_force_field(lbm_lattice* h, const double* force)
 {
     int rc = check_handle(h);
     if (rc) return rc;
+    if ((rc = check_no_open_step(h))) return rc;
     if (!force) return fail(LBM_ERR_INVALID, "null force field");
     if (h->desc.force_mode != LBM_FORCE_FIELD)
         return fail(LBM_ERR_STATE, "lattice was not created with LBM_FORCE_FIELD");
@@ -661,6 +674,7 @@ int lbm_set_porosity(lbm_lattice* h, const float* alpha)
 {
     int rc = check_handle(h);
     if (rc) return rc;
+    if ((rc = check_no_open_step(h))) return rc;
     if (!alpha) return fail(LBM_ERR_INVALID, "null porosity field");
     if (h->desc.force_mode != LBM_FORCE_DRAG)
         return fail(LBM_ERR_STATE, "lattice was not created with LBM_FORCE_DRAG");
@@ -679,6 +693,7 @@ int lbm_set_tau(lbm_lattice* h, double tau)
 {
     int rc = check_handle(h);
     if (rc) return rc;
+    if ((rc = check_no_open_step(h))) return rc;
     if (!(tau > 0.5)) return fail(LBM_ERR_INVALID, "tau must be > 0.5 (got %g)", tau);
     h->desc.tau = tau;
     rebuild_params(h);
@@ -689,6 +704,7 @@ int lbm_set_wall_velocity(lbm_lattice* h, int32_t face, const double* u3)
 {
     int rc = check_handle(h);
     if (rc) return rc;
+    if ((rc = check_no_open_step(h))) return rc;
     if (face < 0 || face > 5 || !u3) return fail(LBM_ERR_INVALID, "bad face index or null velocity");
     for (int a = 0; a < 3; ++a) h->desc.wall_velocity[face][a] = u3[a];
     rebuild_params(h);
@@ -699,6 +715,7 @@ int lbm_set_body_force(lbm_lattice* h, const double* f3)
 {
     int rc = check_handle(h);
     if (rc) return rc;
+    if ((rc = check_no_open_step(h))) return rc;
     if (!f3) return fail(LBM_ERR_INVALID, "null body force");
     for (int a = 0; a < 3; ++a) h->desc.body_force[a] = f3[a];
     rebuild_params(h);
@@ -747,6 +764,7 @@ int lbm_step(lbm_lattice* h, int32_t n_steps)
 {
     int rc = check_handle(h);
     if (rc) return rc;
+    if ((rc = check_no_open_step(h))) return rc;
     if (n_steps < 0) return fail(LBM_ERR_INVALID, "negative step count");
     if ((rc = check_force_ready(h))) return rc;
     int32_t s = 0;
@@ -795,6 +813,59 @@ int lbm_step(lbm_lattice* h, int32_t n_steps)
     return LBM_OK;
 }
 
+int lbm_step_planes(lbm_lattice* h, int32_t x_begin, int32_t x_end)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (h->pre) return fail(LBM_ERR_STATE, "plane-range steps need a stepped state (take the first step with lbm_step)");
+    if (x_begin < 0 || x_end > h->desc.nx || x_begin >= x_end)
+        return fail(LBM_ERR_INVALID, "plane range [%d, %d) outside [0, %d) or empty", x_begin, x_end, h->desc.nx);
+    if ((rc = check_force_ready(h))) return rc;
+    // The register-staged kernel of the lattice's storage and cells per
+    // thread, without outputs, over the window's cells.
+    LaunchArgs a;
+    a.P = h->P;
+    a.P.cell0 = x_begin * h->desc.ny * h->desc.nz;
+    a.P.cell_end = x_end * h->desc.ny * h->desc.nz;
+    a.src = h->buf[h->cur];
+    a.dst = h->buf[h->cur ^ 1];
+    a.post = false;
+    a.f_out = nullptr;
+    a.rho = a.u = nullptr;
+    a.partials = nullptr;
+    a.prev_partials = nullptr;
+    a.prev_count = 0;
+    a.prev_sums = nullptr;
+    a.first = 0;
+    a.count = -1;
+    a.block = h->block;
+    a.vec = h->vec;
+    a.stream = h->stream;
+    a.grid_used = nullptr;
+    a.tma_grid = 0;
+    a.rule_quads = h->rule_quads;
+    for (int k = 0; k < QUAD_KINDS; ++k) a.rule_counts[k] = h->rule_counts[k];
+    a.side = h->side;
+    a.fork = h->ev_fork;
+    a.join = h->ev_join;
+    cudaError_t e = h->storage == LBM_STORAGE_F64 ? launch_exact(KERNEL_STEP, h->desc.force_mode, a)
+                                                  : launch_fast(h->storage, KERNEL_STEP, h->desc.force_mode, a);
+    if (e != cudaSuccess) return cuda_fail(e, "plane-range step launch");
+    h->open_step = true;
+    return LBM_OK;
+}
+
+int lbm_step_commit(lbm_lattice* h)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!h->open_step) return fail(LBM_ERR_STATE, "no plane-range step is open");
+    h->cur ^= 1;
+    h->steps += 1;
+    h->open_step = false;
+    return LBM_OK;
+}
+
 int64_t lbm_step_count(const lbm_lattice* h) { return h ? h->steps : -1; }
 
 int lbm_test_barrier_limit(lbm_lattice* h, int32_t missing_arrivals, int64_t timeout_ns)
@@ -840,6 +911,7 @@ int lbm_set_porosity_dev(lbm_lattice* h, const float* alpha)
 {
     int rc = check_handle(h);
     if (rc) return rc;
+    if ((rc = check_no_open_step(h))) return rc;
     if (!alpha) return fail(LBM_ERR_INVALID, "null porosity field");
     if (h->desc.force_mode != LBM_FORCE_DRAG)
         return fail(LBM_ERR_STATE, "lattice was not created with LBM_FORCE_DRAG");
@@ -863,6 +935,7 @@ int lbm_run_capture(lbm_lattice* h, int32_t n_steps, int32_t every, double* rho_
 {
     int rc = check_handle(h);
     if (rc) return rc;
+    if ((rc = check_no_open_step(h))) return rc;
     if (n_steps < 0 || every < 1) return fail(LBM_ERR_INVALID, "need n_steps >= 0 and every >= 1");
     if (!rho_frames || !u_frames) return fail(LBM_ERR_INVALID, "null frame buffer");
     if ((rc = check_force_ready(h))) return rc;
@@ -889,6 +962,7 @@ int lbm_step_monitor(lbm_lattice* h, int32_t n_steps, double* sums)
 {
     int rc = check_handle(h);
     if (rc) return rc;
+    if ((rc = check_no_open_step(h))) return rc;
     if (n_steps < 0) return fail(LBM_ERR_INVALID, "negative step count");
     if (n_steps > 0 && !sums) return fail(LBM_ERR_INVALID, "null sums array");
     if ((rc = check_force_ready(h))) return rc;

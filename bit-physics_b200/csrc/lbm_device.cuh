@@ -110,7 +110,13 @@ struct Params {
     // from feq_d(1, storage_ref_u), i.e. (f - w_d) - shift_h[d] in f32; zero
     // for the other storages.
     float shift_h[Q];
+    // Cell window of the step kernels (k_step, k_step2, k_step4 with its rule
+    // quads, k_collide_local): they advance the cells [cell0, min(n, cell_end)).
+    int cell0 = 0, cell_end = 0x7fffffff;
 };
+
+// Number of cells in the step kernels' window.
+__host__ __device__ inline int window_cells(const Params& P) { return (P.cell_end < P.n ? P.cell_end : P.n) - P.cell0; }
 
 // np.maximum(rho, 1e-30): NaN propagates.
 __device__ __forceinline__ double rho_safe(double r) { return r != r ? r : (r > 1e-30 ? r : 1e-30); }

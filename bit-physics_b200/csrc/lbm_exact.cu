@@ -34,7 +34,7 @@ template <int FM>
 static cudaError_t launch_exact_fm(int kernel, const LaunchArgs& a)
 {
     using M = ModeExact;
-    const int grid = grid_for(a.P.n, a.block);
+    const int grid = grid_for(kernel == KERNEL_OBSERVE ? a.P.n : window_cells(a.P), a.block);
     if (kernel == KERNEL_OBSERVE) {
         Outputs<double> out{(double*)a.rho, (double*)a.u, a.partials, a.prev_partials, a.prev_count, a.prev_sums,
                           a.first, a.count};

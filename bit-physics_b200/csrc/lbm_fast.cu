@@ -61,7 +61,7 @@ static cudaError_t launch_step4(const LaunchArgs& a, const Streams<typename M::T
         if ((e = cudaEventRecord(a.join, a.side)) != cudaSuccess) return e;
     }
     const int block = a.block < 128 ? a.block : 128;  // the kernel's bound
-    k_step4<M, FM><<<grid_for(a.P.n / 4, block), block, 0, a.stream>>>(a.P, S);
+    k_step4<M, FM><<<grid_for(window_cells(a.P) / 4, block), block, 0, a.stream>>>(a.P, S);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (total > 0) e = cudaStreamWaitEvent(a.stream, a.join, 0);
     return e;
@@ -92,7 +92,7 @@ static cudaError_t launch_step_out(int kernel, const LaunchArgs& a, int grid)
     if (kernel == KERNEL_STEP && a.vec >= 2) {
         // at most the kernel's bound (128 threads for 16-bit storage)
         const int block = a.block < Step2Bounds<T>::threads ? a.block : Step2Bounds<T>::threads;
-        const int grid2 = grid_for(a.P.n / 2, block);
+        const int grid2 = grid_for(window_cells(a.P) / 2, block);
         k_step2<M, FM, OUT><<<grid2, block, 0, a.stream>>>(a.P, S, out);
         if (a.grid_used) *a.grid_used = grid2;
         return cudaGetLastError();
@@ -109,7 +109,7 @@ template <class T, int FM>
 static cudaError_t launch_fast_t(int kernel, const LaunchArgs& a)
 {
     using M = ModeFast<T>;
-    const int grid = grid_for(a.P.n, a.block);
+    const int grid = grid_for(kernel == KERNEL_OBSERVE ? a.P.n : window_cells(a.P), a.block);
     if (kernel == KERNEL_OBSERVE) {
         Outputs<float> out{(float*)a.rho, (float*)a.u, a.partials, a.prev_partials, a.prev_count, a.prev_sums,
                           a.first, a.count};

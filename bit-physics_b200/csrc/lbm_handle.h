@@ -19,6 +19,7 @@ struct lbm_lattice {
     void* buf[2] = {nullptr, nullptr};
     int cur = 0;
     bool pre = true;
+    bool open_step = false;  // lbm_step_planes ran since the last commit
     uint8_t* flags = nullptr;
     uint32_t* bbmask = nullptr; // (n) bounce-back masks, allocated with the flags
     bool has_flags = false;

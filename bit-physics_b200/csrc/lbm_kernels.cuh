@@ -184,9 +184,9 @@ template <class M, int FM, int OUT>
 __global__ void __launch_bounds__(256, 3) k_step(Params P, Streams<typename M::T> S, Outputs<typename M::C> out)
 {
     if constexpr ((OUT & OUT_SUMS) != 0) reduce_prev(out);
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int idx = P.cell0 + blockIdx.x * blockDim.x + threadIdx.x;
     double cons[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    if (idx < P.n) step_single<M, FM, OUT>(P, S, out, idx, cons);
+    if (idx < P.n && idx < P.cell_end) step_single<M, FM, OUT>(P, S, out, idx, cons);
     if constexpr ((OUT & OUT_SUMS) != 0) block_sum5(cons, out.partials + (size_t)blockIdx.x * 5);
 }
 
@@ -401,7 +401,7 @@ __global__ void __launch_bounds__(Step2Bounds<typename M::T>::threads, Step2Boun
                                                                     Outputs<typename M::C> out)
 {
     if constexpr ((OUT & OUT_SUMS) != 0) reduce_prev(out);
-    const int idx0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+    const int idx0 = P.cell0 + 2 * (blockIdx.x * blockDim.x + threadIdx.x);
     double cons[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     if constexpr ((OUT & OUT_SUMS) != 0) {
         // Threads past the end compute the last pair again, store nothing and
@@ -412,7 +412,7 @@ __global__ void __launch_bounds__(Step2Bounds<typename M::T>::threads, Step2Boun
         step_pair<M, FM, OUT>(P, S, out, live ? idx0 : P.n - 2, cons, live);
         block_sum5(cons, out.partials + (size_t)blockIdx.x * 5);
     } else {
-        if (idx0 < P.n) step_pair<M, FM, OUT>(P, S, out, idx0, cons);
+        if (idx0 < P.n && idx0 < P.cell_end) step_pair<M, FM, OUT>(P, S, out, idx0, cons);
     }
 }
 
@@ -615,8 +615,8 @@ __global__ void __launch_bounds__(128, 4) k_step4(Params P, Streams<typename M::
 {
     using T = typename M::T;
     static_assert(sizeof(T) == 2, "k_step4: 16-bit storage only");
-    const int idx0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
-    if (idx0 >= P.n) return;
+    const int idx0 = P.cell0 + 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (idx0 >= P.n || idx0 >= P.cell_end) return;
     int x, y, z0;
     decode_xyz(P, idx0, x, y, z0);
     const Nbr nb0 = make_nbr(P, x, y, z0);
@@ -676,6 +676,7 @@ __device__ __forceinline__ void rule_pair(const Params& P, const Streams<typenam
     using T = typename M::T;
     if (k < 2 * n_near) {
         const int idx0 = 4 * near_q[k >> 1] + 2 * (k & 1);
+        if (idx0 < P.cell0 || idx0 >= P.cell_end) return;
         int x, y, z0;
         decode_xyz(P, idx0, x, y, z0);
         const Nbr nb0 = make_nbr(P, x, y, z0);
@@ -702,6 +703,7 @@ __device__ __forceinline__ void rule_pair(const Params& P, const Streams<typenam
     k -= 2 * n_near;
     if (k < 2 * n_out) {
         const int idx0 = 4 * out_q[k >> 1] + 2 * (k & 1);
+        if (idx0 < P.cell0 || idx0 >= P.cell_end) return;
         int x, y, z0;
         decode_xyz(P, idx0, x, y, z0);
         const int gx = x == 0 ? P.nx - 1 : x - 1;
@@ -713,8 +715,10 @@ __device__ __forceinline__ void rule_pair(const Params& P, const Streams<typenam
     }
     k -= 2 * n_out;
     if (k >= 2 * n_other) return;
+    const int idx0 = 4 * other_q[k >> 1] + 2 * (k & 1);
+    if (idx0 < P.cell0 || idx0 >= P.cell_end) return;
     const Outputs<float> none{nullptr, nullptr, nullptr};
-    step_pair<M, FM, OUT_NONE>(P, S, none, 4 * other_q[k >> 1] + 2 * (k & 1), nullptr);
+    step_pair<M, FM, OUT_NONE>(P, S, none, idx0, nullptr);
 }
 
 // The rule quads of k_step4 in a grid-stride loop over the pair tasks.  The
@@ -847,9 +851,9 @@ __global__ void __launch_bounds__(256) k_collide_local(Params P, Streams<typenam
                                                        Outputs<typename M::C> out)
 {
     if constexpr ((OUT & OUT_SUMS) != 0) reduce_prev(out);
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int idx = P.cell0 + blockIdx.x * blockDim.x + threadIdx.x;
     double cons[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    if (idx < P.n) collide_single<M, FM, OUT>(P, S, out, idx, cons);
+    if (idx < P.n && idx < P.cell_end) collide_single<M, FM, OUT>(P, S, out, idx, cons);
     if constexpr ((OUT & OUT_SUMS) != 0) block_sum5(cons, out.partials + (size_t)blockIdx.x * 5);
 }
 

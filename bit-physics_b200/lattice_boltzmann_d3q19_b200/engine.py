@@ -200,6 +200,18 @@ class Lattice:
     def step(self, n_steps: int = 1) -> None:
         N.check(N.lib().lbm_step(self._h, int(n_steps)))
 
+    def step_planes(self, x_begin: int, x_end: int) -> None:
+        """Advance the x-planes [x_begin, x_end) of the current step into the
+        next state (enqueued on the lattice's stream); step_commit() ends the
+        step.  Until then the current state is the step's source, which
+        plane_get_device / plane_put_device read and write; planes not
+        advanced hold unspecified values after the commit.  Needs a stepped
+        state (the first step after a state upload is a step())."""
+        N.check(N.lib().lbm_step_planes(self._h, int(x_begin), int(x_end)))
+
+    def step_commit(self) -> None:
+        N.check(N.lib().lbm_step_commit(self._h))
+
     @property
     def step_count(self) -> int:
         return int(N.lib().lbm_step_count(self._h))

@@ -149,6 +149,23 @@ int lbm_set_body_force(lbm_lattice* h, const double* f3);
 int lbm_step(lbm_lattice* h, int32_t n_steps);
 int64_t lbm_step_count(const lbm_lattice* h);
 
+/* One step split over several launches (no reference counterpart: the
+ * reference steps one whole lattice per call).  lbm_step_planes advances
+ * the x-planes [x_begin, x_end) of the current step into the next state;
+ * lbm_step_commit ends the step and makes the next state current.  Until the
+ * commit the current state is the step's source: readbacks and
+ * lbm_plane_get / lbm_plane_put act on it (a halo plane filled by
+ * lbm_plane_put before the planes next to it are advanced is what they
+ * pull), and calls that change the state or the parameters return
+ * LBM_ERR_STATE.  Planes left out hold unspecified values after the
+ * commit.  Needs a stepped state (LBM_ERR_STATE right after a state upload:
+ * take that step with lbm_step).  Runs the register-staged kernel of the
+ * lattice's storage and cells per thread on its stream: the advanced planes
+ * are bit-identical to lbm_step's result under automatic, register or
+ * pipelined staging. */
+int lbm_step_planes(lbm_lattice* h, int32_t x_begin, int32_t x_end);
+int lbm_step_commit(lbm_lattice* h);
+
 /* rho and u of the current state: density_field + macroscopic_velocity
  * (d3q19_warp.py:283-292, :371-383).  Either pointer may be NULL. */
 int lbm_get_rho_u(lbm_lattice* h, double* rho, double* u);

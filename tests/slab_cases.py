@@ -22,7 +22,7 @@ class OracleEngine:
     def _dirs(mask):
         return [d for d in range(19) if (mask >> d) & 1]
 
-    def plane_get(self, x, mask):
+    def plane_get(self, x, mask, slot=None):
         return np.ascontiguousarray(self.lat._a[self._dirs(mask), x])
 
     def plane_put(self, x, mask, buf):
@@ -47,7 +47,30 @@ class OracleEngine:
         return np.array([f.sum(0)[keep].sum()] + [np.tensordot(c[:, a], f, 1)[keep].sum() for a in range(3)])
 
 
-def oracle_slab(c, x0, x1):
+class OracleSplitEngine(OracleEngine):
+    """OracleEngine with plane-range steps: step_planes computes the step
+    of the whole slab from the current state and keeps the planes asked
+    for; planes never advanced before the commit are NaN in the new state,
+    so a step that read one would show it."""
+
+    def __init__(self, lat, flags):
+        super().__init__(lat, flags)
+        self._next = None
+
+    def step_planes(self, x0, x1):
+        assert not self.lat._pre, "plane-range steps need a stepped state"
+        full = np.empty_like(self.lat._a)
+        O.lib().orc_engine_step(self.lat._L, O._ptr(self.lat._a), O._ptr(full), None, None)
+        if self._next is None:
+            self._next = np.full_like(self.lat._a, np.nan)
+        self._next[:, x0:x1] = full[:, x0:x1]
+
+    def step_commit(self):
+        self.lat._a, self._next = self._next, None
+        self.lat._spare = None
+
+
+def oracle_slab(c, x0, x1, split=False):
     """SlabLattice of an adjoint_cases case (x periodic) on the oracle."""
     nx = c["shape"][0]
     kw = c["kw"]
@@ -58,4 +81,5 @@ def oracle_slab(c, x0, x1):
                           wall_velocity=kw.get("wall_velocity"), flags=flags, force_mode=FORCE[kw["force_mode"]],
                           body_force=kw.get("body_force", (0.0, 0.0, 0.0)), force_field=force, porosity=alpha,
                           drag_k=kw.get("drag_k", 0.0), inflow_u=kw.get("inflow_u", (0, 0, 0)))
-    return SlabLattice(OracleEngine(lat, flags), x0, x1, flags=c["flags"], nx=nx)
+    engine = (OracleSplitEngine if split else OracleEngine)(lat, flags)
+    return SlabLattice(engine, x0, x1, flags=c["flags"], nx=nx)

@@ -15,7 +15,7 @@ import torch.multiprocessing as mp
 from adjoint_cases import case, oracle_lattice
 from slab_cases import oracle_slab
 
-from lattice_boltzmann_d3q19_b200.slab import SlabGroup, exchange_distributed, slab_bounds, with_halos
+from lattice_boltzmann_d3q19_b200.slab import SlabGroup, exchange_distributed, slab_bounds, step_distributed, with_halos
 
 
 def test_slab_bounds_and_halos():
@@ -34,15 +34,18 @@ def test_outflow_on_a_slab_face_is_refused():
         oracle_slab(c, 18, 20)
 
 
+@pytest.mark.parametrize("split", [False, True], ids=["whole-slab", "overlapped"])
 @pytest.mark.parametrize("name,parts", [("drag_channel", 3), ("field_periodic", 2)])
-def test_slab_group_matches_unsplit(name, parts):
+def test_slab_group_matches_unsplit(name, parts, split):
+    """Whole-slab steps after an exchange, and the overlapped step (interior,
+    then imported halos and boundary planes; halo planes never advanced)."""
     c = case(name)
     n_steps = 7
     ref = oracle_lattice(c)
     ref.set_populations(c["f0"])
     ref.step(n_steps)
     rho_ref, u_ref = ref.rho_u()
-    group = SlabGroup([oracle_slab(c, x0, x1) for x0, x1 in slab_bounds(c["shape"][0], parts)])
+    group = SlabGroup([oracle_slab(c, x0, x1, split) for x0, x1 in slab_bounds(c["shape"][0], parts)])
     for s in group.slabs:
         s.set_populations(c["f0"])
     group.step(n_steps)
@@ -58,18 +61,21 @@ def _free_port() -> int:
         return s.getsockname()[1]
 
 
-def _rank_main(rank, world, port, n_steps, out_dir):
+def _rank_main(rank, world, port, n_steps, out_dir, split):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=__import__("datetime").timedelta(seconds=60))
     try:
         c = case("drag_channel")
         x0, x1 = slab_bounds(c["shape"][0], world)[rank]
-        s = oracle_slab(c, x0, x1)
+        s = oracle_slab(c, x0, x1, split)
         s.set_populations(c["f0"])
         to_t = lambda b: torch.from_numpy(np.ascontiguousarray(b))  # noqa: E731
         from_t = lambda t, like: t.numpy().reshape(like.shape)  # noqa: E731
         for k in range(n_steps):
+            if split:
+                step_distributed(s, rank, world, None, to_t, from_t)
+                continue
             if k > 0:
                 exchange_distributed(s, rank, world, to_t, from_t)
             s.engine.step(1)
@@ -80,14 +86,17 @@ def _rank_main(rank, world, port, n_steps, out_dir):
         dist.destroy_process_group()
 
 
-def test_two_gloo_ranks_match_unsplit(tmp_path):
+@pytest.mark.parametrize("split", [False, True], ids=["whole-slab", "overlapped"])
+def test_two_gloo_ranks_match_unsplit(tmp_path, split):
     """world_size 2 over gloo on the CPU: each rank steps one oracle slab and
-    exchanges its faces with exchange_distributed (the code path NCCL runs on
-    GPUs); the gathered owned planes equal the unsplit oracle's."""
+    exchanges its faces with exchange_distributed, or takes the overlapped
+    step_distributed (the code paths NCCL runs on GPUs); the gathered owned
+    planes equal the unsplit oracle's."""
     n_steps, world = 6, 2
     ctx = mp.get_context("spawn")
     port = _free_port()
-    procs = [ctx.Process(target=_rank_main, args=(r, world, port, n_steps, str(tmp_path))) for r in range(world)]
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, n_steps, str(tmp_path), split))
+             for r in range(world)]
     for p in procs:
         p.start()
     for p in procs:
