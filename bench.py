@@ -571,6 +571,17 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                     "pinned f64 arrays, wall clock",
             "mass_drift_rel": float((sums[-1, 0] - sums[0, 0]) / sums[0, 0]),
         }
+    # strong scaling of the same channel by x-slabs (one slab per rank, the
+    # overlapped step; one rank exchanges with itself)
+    slab = None
+    if not args.skip_slab:
+        slab_args = argparse.Namespace(steps=min(args.steps, 1000), warmup=args.warmup)
+        ms, slab_healthy, planes = slab_leg(slab_args, rank, world, local_rank, args.storage, True)
+        slab = {"value": n * slab_args.steps / (ms / 1e3) / 1e9, "unit": "GLUPS", "scaling": "strong",
+                "ms_per_step": ms / slab_args.steps, "steps": slab_args.steps, "slabs": world,
+                "planes_per_slab": planes, "healthy": slab_healthy,
+                "what": "the channel split in x over the ranks, one halo plane per side, faces exchanged by "
+                        "NCCL point-to-point on a second stream while the interior planes step"}
     sampler.stop()
     if nvml is not None:
         nvml.stop()
@@ -627,6 +638,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "variants": variants,
         "precision": precision,
         "adjoint_over_forward": adjoint,
+        "slab_strong_scaling": slab,
     }
     print(json.dumps(line), flush=True)
 
@@ -765,7 +777,8 @@ def run_ensemble(args):
     """64 independent lid-driven cavities, sizes U[32,128] per axis, tau
     U[0.52,0.9], lid U[0.02,0.08] (seed 42), f16 deviation storage: one
     launch per lattice and step, one batched launch per step (default
-    schedule), and the autotuned schedule."""
+    schedule), each lattice's own kernels on 8 parallel graph branches, and
+    the autotuned schedule."""
     import torch
 
     from lattice_boltzmann_d3q19_b200 import Batch, geometry
@@ -797,6 +810,11 @@ def run_ensemble(args):
         dt = timed(lambda: b.step(args.steps))
         out["batched_default"] = {"glups": cells * args.steps / dt / 1e9, "schedule": list(b.schedule()),
                                   "launches_per_step": 1}
+        b.set_schedule("branches", 128, 8)
+        b.step(2)
+        dt = timed(lambda: b.step(args.steps))
+        out["batched_branches"] = {"glups": cells * args.steps / dt / 1e9, "schedule": list(b.schedule()),
+                                   "launches_per_step": "one graph of per-lattice kernels per two steps"}
         ms = b.autotune(20)
         b.step(2)
         dt = timed(lambda: b.step(args.steps))
@@ -845,20 +863,39 @@ def slab_leg(args, rank: int, world: int, local_rank: int, storage: str, overlap
                 lat.step(1)
                 slab.stepped = True
 
-        advance(args.warmup)
+        advance(max(args.warmup, 2))
+        # One rank: two steps captured into a CUDA graph and replayed (the
+        # enqueueing of a split step's launches from Python would otherwise
+        # set the pace); several ranks step eagerly (NCCL point-to-point).
+        graph = None
+        if world == 1:
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph, stream=stream, capture_error_mode="relaxed"):
+                advance(2)
+            graph.replay()
+        steps = args.steps + args.steps % 2 if graph is not None else args.steps
+
+        def run():
+            if graph is None:
+                advance(steps)
+            else:
+                for _ in range(steps // 2):
+                    graph.replay()
+
         start = torch.cuda.Event(enable_timing=True)
         end = torch.cuda.Event(enable_timing=True)
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
         start.record(stream)
-        advance(args.steps)
+        run()
         end.record(stream)
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
-        ms = start.elapsed_time(end)
+        ms = start.elapsed_time(end) * args.steps / steps
         healthy = lat.check_health()
+        del graph
         lat.close()
     if world > 1:
         t = torch.tensor([ms], device=f"cuda:{local_rank}", dtype=torch.float64)
@@ -1087,6 +1124,7 @@ def main():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-adjoint", action="store_true")
+    ap.add_argument("--skip-slab", action="store_true")
     ap.add_argument("--precision", default="c3", choices=["c3", "c2", "none"],
                     help="5000-step error leg: 512x256x256 (c3), the headline 256x128x128 (c2) or none")
     ap.add_argument("--repeats", type=int, default=REPEATS)

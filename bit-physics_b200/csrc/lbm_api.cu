@@ -1,5 +1,6 @@
 // lbm_api.cu -- the C ABI of include/lbm_d3q19.h: lattice handles, state
 // transfer, the step loop and the stateless reference functions.
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -89,6 +90,8 @@ void init_geometry(Params& P, int nx, int ny, int nz)
     P.ny = ny;
     P.nz = nz;
     P.n = nx * ny * nz;
+    P.cell0 = 0;  // the step kernels' window: every cell
+    P.cell_end = P.n;
     P.nynz = ny * nz;
     P.div_nz.init((uint32_t)nz);
     P.div_ny.init((uint32_t)ny);
@@ -1398,6 +1401,16 @@ struct lbm_batch {
     int sms = 1;
     cudaGraphExec_t graph = nullptr;
     bool graph_valid = false;
+    // SCHED_BRANCHES: `grid` streams; lattice i steps on branches[branch_of[i]]
+    // (largest lattices first, each to the branch with the fewest cells).  The
+    // two-step graph holds every lattice's buffers and parameters: it is
+    // recaptured when a lattice's buffer parity or parameters differ from
+    // the capture's.
+    std::vector<cudaStream_t> branches;
+    std::vector<cudaEvent_t> branch_done;
+    cudaEvent_t root = nullptr;
+    std::vector<int> branch_of, branch_order;
+    std::vector<int> graph_cur, graph_params;
 };
 
 namespace {
@@ -1407,8 +1420,17 @@ int batch_span(const lbm_batch* b) { return b->block * (b->sched == SCHED_SINGLE
 int batch_build_items(lbm_batch* b)
 {
     const int span = batch_span(b);
+    // Lattices by kind (even nz, which the pair schedules step with vector
+    // access, before odd nz), then by size: neighbouring blocks run items
+    // of one kind at a time.
+    std::vector<int> order(b->count);
+    for (int i = 0; i < b->count; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int i, int j) {
+        const int oi = b->lats[i]->desc.nz % 2, oj = b->lats[j]->desc.nz % 2;
+        return oi != oj ? oi < oj : b->lats[i]->n > b->lats[j]->n;
+    });
     std::vector<BatchItem> items;
-    for (int i = 0; i < b->count; ++i)
+    for (int i : order)
         for (int c = 0; c < b->lats[i]->n; c += span) items.push_back(BatchItem{i, c});
     if ((int)items.size() > b->items_cap) {
         if (b->items) CK(cudaFree(b->items), "batch items free");
@@ -1429,8 +1451,81 @@ int batch_build_items(lbm_batch* b)
 
 int batch_grid(const lbm_batch* b)
 {
+    if (b->sched == SCHED_BRANCHES) return b->grid > 0 ? b->grid : 8;
     const int g = b->grid > 0 ? b->grid : 4 * b->sms;
     return g < b->nitems ? g : b->nitems;
+}
+
+void batch_free_branches(lbm_batch* b)
+{
+    for (cudaStream_t s : b->branches) cudaStreamDestroy(s);
+    for (cudaEvent_t e : b->branch_done) cudaEventDestroy(e);
+    b->branches.clear();
+    b->branch_done.clear();
+}
+
+// Streams, events and the lattice -> branch assignment of SCHED_BRANCHES.
+int batch_build_branches(lbm_batch* b, int nb)
+{
+    if ((int)b->branches.size() != nb) {
+        CK(cudaStreamSynchronize(b->stream), "batch sync");
+        batch_free_branches(b);
+        for (int k = 0; k < nb; ++k) {
+            cudaStream_t s = nullptr;
+            cudaEvent_t e = nullptr;
+            CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "branch stream");
+            b->branches.push_back(s);
+            CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "branch event");
+            b->branch_done.push_back(e);
+        }
+    }
+    if (!b->root) CK(cudaEventCreateWithFlags(&b->root, cudaEventDisableTiming), "root event");
+    b->branch_order.resize(b->count);
+    for (int i = 0; i < b->count; ++i) b->branch_order[i] = i;
+    std::stable_sort(b->branch_order.begin(), b->branch_order.end(),
+                     [&](int i, int j) { return b->lats[i]->n > b->lats[j]->n; });
+    std::vector<long long> load(nb, 0);
+    b->branch_of.assign(b->count, 0);
+    for (int i : b->branch_order) {
+        int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        b->branch_of[i] = k;
+        load[k] += b->lats[i]->n;
+    }
+    return LBM_OK;
+}
+
+// One step of every lattice (phase 0: buf[cur] -> buf[cur ^ 1], phase 1 the
+// reverse) with each lattice's own kernels on its branch, forked from and
+// joined into the batch stream.
+cudaError_t batch_branch_step(lbm_batch* b, int phase)
+{
+    cudaError_t e;
+    if ((e = cudaEventRecord(b->root, b->stream)) != cudaSuccess) return e;
+    const int nb = (int)b->branches.size();
+    for (int k = 0; k < nb; ++k)
+        if ((e = cudaStreamWaitEvent(b->branches[k], b->root, 0)) != cudaSuccess) return e;
+    for (int i : b->branch_order) {
+        lbm_lattice* h = b->lats[i];
+        const int c = h->cur ^ phase;
+        cudaStream_t own = h->stream;
+        h->stream = b->branches[b->branch_of[i]];
+        e = launch(h, KERNEL_STEP, h->buf[c], h->buf[c ^ 1], false, nullptr, nullptr, nullptr, nullptr);
+        h->stream = own;
+        if (e != cudaSuccess) return e;
+    }
+    for (int k = 0; k < nb; ++k) {
+        if ((e = cudaEventRecord(b->branch_done[k], b->branches[k])) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(b->stream, b->branch_done[k], 0)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+bool batch_branch_graph_current(const lbm_batch* b)
+{
+    if (!b->graph_valid || (int)b->graph_cur.size() != b->count) return false;
+    for (int i = 0; i < b->count; ++i)
+        if (b->graph_cur[i] != b->lats[i]->cur || b->graph_params[i] != b->lats[i]->params_version) return false;
+    return true;
 }
 
 // Records for the next steps: phase 0 reads buf[cur], phase 1 the other.
@@ -1531,6 +1626,8 @@ int lbm_batch_destroy(lbm_batch* b)
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->graph) cudaGraphExecDestroy(b->graph);
+    batch_free_branches(b);
+    if (b->root) cudaEventDestroy(b->root);
     for (lbm_lattice* h : b->lats) {
         h->stream = nullptr;  // the batch owns the stream
         h->own_stream = false;
@@ -1555,16 +1652,19 @@ int lbm_batch_lattice(lbm_batch* b, int32_t i, lbm_lattice** out)
 int lbm_batch_set_schedule(lbm_batch* b, int32_t sched, int32_t block, int32_t grid)
 {
     if (!b) return fail(LBM_ERR_INVALID, "null batch handle");
-    if (sched < SCHED_SINGLE || sched > SCHED_PAIR_MIXED) return fail(LBM_ERR_INVALID, "unknown schedule %d", sched);
-    if (sched != SCHED_SINGLE && (b->storage == LBM_STORAGE_F64 || b->force_mode == LBM_FORCE_FIELD ||
-                                  b->force_mode == LBM_FORCE_DRAG))
+    if (sched < SCHED_SINGLE || sched > SCHED_BRANCHES) return fail(LBM_ERR_INVALID, "unknown schedule %d", sched);
+    if ((sched == SCHED_PAIR_SCALAR || sched == SCHED_PAIR_MIXED) &&
+        (b->storage == LBM_STORAGE_F64 || b->force_mode == LBM_FORCE_FIELD || b->force_mode == LBM_FORCE_DRAG))
         return fail(LBM_ERR_UNSUPPORTED, "two-cell schedules need f32/f16/bf16 storage and no per-cell force");
     if (block < 32 || block > 256 || block % 32) return fail(LBM_ERR_INVALID, "block must be a multiple of 32 <= 256");
     if (grid < 0) return fail(LBM_ERR_INVALID, "negative grid");
+    if (sched == SCHED_BRANCHES && grid > 64) return fail(LBM_ERR_INVALID, "at most 64 branches");
     CK(cudaSetDevice(b->device), "cudaSetDevice");
     b->sched = sched;
     b->block = block;
     b->grid = grid;
+    int rc;
+    if (sched == SCHED_BRANCHES && (rc = batch_build_branches(b, batch_grid(b)))) return rc;
     return batch_build_items(b);
 }
 
@@ -1608,6 +1708,36 @@ int lbm_batch_step(lbm_batch* b, int32_t n_steps)
     }
     const int rest = n_steps - done;
     if (rest <= 0) return LBM_OK;
+    if (b->sched == SCHED_BRANCHES) {
+        if (rest >= 2 && !batch_branch_graph_current(b)) {
+            if (b->graph) cudaGraphExecDestroy(b->graph);
+            b->graph = nullptr;
+            b->graph_valid = false;
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "graph capture begin");
+            cudaError_t e0 = batch_branch_step(b, 0);
+            cudaError_t e1 = e0 == cudaSuccess ? batch_branch_step(b, 1) : e0;
+            cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+            if (e0 != cudaSuccess || e1 != cudaSuccess || e2 != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                return cuda_fail(e0 != cudaSuccess ? e0 : (e1 != cudaSuccess ? e1 : e2), "branch graph capture");
+            }
+            cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return cuda_fail(e, "branch graph instantiate");
+            b->graph_valid = true;
+            b->graph_cur.resize(b->count);
+            b->graph_params.resize(b->count);
+            for (int i = 0; i < b->count; ++i) {
+                b->graph_cur[i] = b->lats[i]->cur;
+                b->graph_params[i] = b->lats[i]->params_version;
+            }
+        }
+        for (int k = 0; k + 1 < rest; k += 2) CK(cudaGraphLaunch(b->graph, b->stream), "branch graph launch");
+        if (rest % 2) CK(batch_branch_step(b, 0), "branch step launch");
+        batch_advance_bookkeeping(b, rest);
+        return LBM_OK;
+    }
     if ((rc = batch_upload_records(b))) return rc;
     if (rest >= 2 && !b->graph_valid) {
         cudaGraph_t g = nullptr;
@@ -1683,10 +1813,14 @@ int lbm_batch_autotune(lbm_batch* b, int32_t trial_steps, double* best_ms)
         cudaEvent_t e0, e1;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
+        scheds.push_back(SCHED_BRANCHES);
         for (int sc : scheds)
             for (int blk : {128, 256})
                 for (int per_sm : {2, 4, 8}) {
-                    if ((rc = lbm_batch_set_schedule(b, sc, blk, per_sm * b->sms))) break;
+                    // SCHED_BRANCHES: 4, 8 or 16 branches, once (the block size is each lattice's own)
+                    if (sc == SCHED_BRANCHES && blk != 128) continue;
+                    const int g = sc == SCHED_BRANCHES ? 2 * per_sm : per_sm * b->sms;
+                    if ((rc = lbm_batch_set_schedule(b, sc, blk, g))) break;
                     if ((rc = lbm_batch_step(b, 2))) break;  // capture + warm
                     cudaEventRecord(e0, b->stream);
                     if ((rc = lbm_batch_step(b, trial_steps))) break;
@@ -1699,7 +1833,7 @@ int lbm_batch_autotune(lbm_batch* b, int32_t trial_steps, double* best_ms)
                         best = per;
                         bs = sc;
                         bb = blk;
-                        bg = per_sm * b->sms;
+                        bg = g;
                     }
                 }
         cudaEventDestroy(e0);

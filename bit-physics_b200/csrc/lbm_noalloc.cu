@@ -115,6 +115,8 @@ extern "C" int lbm_conservation_noalloc(const double* f, const uint8_t* flags, i
     P.ny = ny;
     P.nz = nz;
     P.n = (int)n;
+    P.cell0 = 0;
+    P.cell_end = P.n;
     P.nynz = ny * nz;
     P.div_nz.init((uint32_t)nz);
     P.div_ny.init((uint32_t)ny);

@@ -28,7 +28,7 @@ STORAGE = {"f64": 0, "f32": 1, "f16": 2, "bf16": 3}
 FORCE = {"none": 0, "uniform": 1, "field": 2, "drag": 3}
 FACES = {"x-": 0, "x+": 1, "y-": 2, "y+": 3, "z-": 4, "z+": 5}
 STAGING = {"auto": 0, "registers": 1, "tma": 2, "pipelined": 3, "persistent": 4}
-SCHEDULES = {"single": 0, "pair_scalar": 1, "pair_mixed": 2}
+SCHEDULES = {"single": 0, "pair_scalar": 1, "pair_mixed": 2, "branches": 3}
 CELL_FLUID, CELL_SOLID, CELL_INFLOW, CELL_OUTFLOW = 0, 1, 2, 3
 
 

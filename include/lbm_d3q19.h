@@ -240,6 +240,10 @@ typedef struct lbm_batch lbm_batch;
 #define LBM_SCHED_SINGLE 0      /* one cell per thread                              */
 #define LBM_SCHED_PAIR_SCALAR 1 /* two cells per thread, f32x2 collision            */
 #define LBM_SCHED_PAIR_MIXED 2  /* as 1, vector memory access where nz is even      */
+#define LBM_SCHED_BRANCHES 3    /* no batched kernel: every lattice's own step
+                                   kernels on `grid` parallel streams (0: 8),
+                                   largest lattices first, each to the stream with
+                                   the fewest cells; two steps per captured graph  */
 
 int lbm_batch_create(const lbm_desc* descs, int32_t count, lbm_batch** out);
 int lbm_batch_destroy(lbm_batch* b);
@@ -247,10 +251,13 @@ int lbm_batch_count(const lbm_batch* b);
 /* Borrowed handle of lattice i (valid until lbm_batch_destroy). */
 int lbm_batch_lattice(lbm_batch* b, int32_t i, lbm_lattice** out);
 /* Work schedule: sched LBM_SCHED_*, threads per block (multiple of 32, <= 256),
- * grid = blocks of the persistent launch (0: 4 per SM). */
+ * grid = blocks of the persistent launch (0: 4 per SM); for
+ * LBM_SCHED_BRANCHES grid is the number of streams (<= 64) and block is
+ * unused. */
 int lbm_batch_set_schedule(lbm_batch* b, int32_t sched, int32_t block, int32_t grid);
 int lbm_batch_get_schedule(const lbm_batch* b, int32_t* sched, int32_t* block, int32_t* grid);
-/* Advance every lattice n_steps: one launch per step, steady-state steps
+/* Advance every lattice n_steps: one launch per step (LBM_SCHED_BRANCHES:
+ * one graph of per-lattice launches per two steps), steady-state steps
  * replayed from a captured two-step CUDA graph. */
 int lbm_batch_step(lbm_batch* b, int32_t n_steps);
 /* The same with one launch per lattice and step (for comparison). */

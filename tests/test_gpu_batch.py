@@ -99,11 +99,40 @@ def test_unbatched_equals_batched_and_autotune_restores_state():
         ms = a.autotune(4)
         assert ms > 0.0
         sched = a.schedule()
-        assert sched[0] in ("single", "pair_scalar", "pair_mixed")
+        assert sched[0] in ("single", "pair_scalar", "pair_mixed", "branches")
         for k in range(len(specs)):
             assert same_bytes(a[k].get_populations(), before[k])
             assert a[k].step_count == counts[k]
         a.step(5)  # still steps with the chosen schedule
+
+
+@pytest.mark.parametrize("storage", ["f64", "f32", "f16"])
+def test_branch_schedule_equals_unbatched(storage):
+    """LBM_SCHED_BRANCHES runs every lattice's own kernels (four-cell ones
+    with their rule quads where nz % 4 == 0): bit-identical to one launch
+    per lattice, through graph replays, an odd remainder, a parameter
+    change and a lattice stepped on its own (both recapture the graph)."""
+    specs = _specs(storage)
+    states = [random_state(sp["shape"], 80 + k, amp=0.01) for k, sp in enumerate(specs)]
+    with Batch(specs) as a, Batch(specs) as b:
+        for k, f in enumerate(states):
+            a[k].set_populations(f)
+            b[k].set_populations(f)
+        a.set_schedule("branches", 128, 3)
+        assert a.schedule() == ("branches", 128, 3)
+        a.step(8)
+        b.step_unbatched(8)
+        a[2].set_tau(0.65)
+        b[2].set_tau(0.65)
+        a.step(5)
+        b.step_unbatched(5)
+        a[1].step(1)
+        b[1].step(1)
+        a.step(6)
+        b.step_unbatched(6)
+        for k in range(len(specs)):
+            assert same_bytes(a[k].get_populations(), b[k].get_populations()), k
+            assert a[k].step_count == b[k].step_count
 
 
 def test_batch_rejects_mixed_storage_and_bad_schedule():
@@ -114,3 +143,5 @@ def test_batch_rejects_mixed_storage_and_bad_schedule():
     with Batch(_specs("f64")) as b:
         with pytest.raises(LbmError):
             b.set_schedule("pair_scalar")
+        with pytest.raises(LbmError):
+            b.set_schedule("branches", 128, 65)
