@@ -189,9 +189,8 @@ cudaError_t lbm::api::launch(lbm_lattice* h, int kernel, const void* src, void* 
     a.sums_grid = kernel == KERNEL_STEP ? h->sums_grid : 0;
     a.rule_quads = h->rule_quads;
     for (int k = 0; k < QUAD_KINDS; ++k) a.rule_counts[k] = h->rule_counts[k];
-    a.side = h->side;
-    a.fork = h->ev_fork;
-    a.join = h->ev_join;
+    a.rules_grid = h->rules_grid;
+    if (kernel == KERNEL_STEP && !rho && !u && !partials) a.P.order = h->order;
     if (kernel == KERNEL_STEP && h->use_tma) {
         a.tma_grid = h->tma_grid;
         a.tile = h->tile;
@@ -214,6 +213,13 @@ int refresh_rule_quads(lbm_lattice* h)
     CK(cudaMemcpyAsync(h->rule_counts, counts, sizeof(int) * QUAD_KINDS, cudaMemcpyDeviceToHost, h->stream),
        "rule quad counts");
     CK(cudaStreamSynchronize(h->stream), "rule quad sync");
+    // Leading blocks of k_step4: about as many rule tasks per thread as the
+    // plain quads take waves of resident blocks (4 of 128 threads per SM),
+    // so that the rule blocks finish with the plain ones.
+    const long long total = (long long)h->rule_counts[0] + h->rule_counts[1] + h->rule_counts[2];
+    const long long plain = (long long)cap - total > 0 ? (long long)cap - total : 1;
+    const long long want = (2 * total * 4 * h->sms + plain - 1) / plain;
+    h->rules_grid = total > 0 ? (int)(want < 1 ? 1 : (want > 4 * h->sms ? 4 * h->sms : want)) : 0;
     h->params_version += 1;  // a captured step graph holds the old count
     return LBM_OK;
 }
@@ -475,13 +481,29 @@ int lbm_create(const lbm_desc* desc, lbm_lattice** out)
     }
     if (h->vec == 4) {
         e = cudaMalloc((void**)&h->rule_quads, sizeof(int) * ((size_t)QUAD_KINDS * (h->n / 4) + QUAD_KINDS));
-        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming);
         if (e != cudaSuccess) return cleanup(cuda_fail(e, "four-cell step set-up"));
+        if (cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, desc->device) != cudaSuccess ||
+            h->sms < 1)
+            h->sms = 1;
     }
     rebuild_params(h);
     if (int rc2 = refresh_rule_quads(h)) return cleanup(rc2);
+    // Visit order of the plain one- and two-cell steps on a lattice with
+    // walls: interior items first, then those on the walled faces (fixed by
+    // the periodicity, which does not change after creation).
+    if (h->vec <= 2 && desc->periodic != 7) {
+        const size_t items = (size_t)h->n / h->vec;
+        e = cudaMalloc((void**)&h->order, sizeof(int) * (items + 1));
+        if (e == cudaSuccess) e = launch_face_order(h->P, h->vec, h->order, h->order + items, h->stream);
+        int faces = -1;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&faces, h->order + items, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) return cleanup(cuda_fail(e, "face order"));
+        const long long bx = desc->nx - 2 * (int)h->P.walled[0], by = desc->ny - 2 * (int)h->P.walled[1],
+                        bz = desc->nz / h->vec - 2 * (int)h->P.walled[2];
+        const long long inner = bx > 0 && by > 0 && bz > 0 ? bx * by * bz : 0;
+        if (faces != (long long)items - inner) return cleanup(fail(LBM_ERR_CUDA, "face order incomplete"));
+    }
     // Rest state f = w_i (rho = 1, u = 0).
     e = launch_feq_init(h->storage, h->P, nullptr, nullptr, h->buf[0], h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -498,15 +520,11 @@ int lbm_destroy(lbm_lattice* h)
     cudaSetDevice(h->desc.device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->graph) cudaGraphExecDestroy(h->graph);
-    if (h->side) cudaStreamSynchronize(h->side);
     void* ptrs[] = {h->buf[0], h->buf[1], h->flags, h->bbmask, h->force, h->poro, h->rho,
                     h->u, h->partials, h->sums, h->staging, h->monitor, h->err, h->diag, h->rule_quads, h->bar,
-                    h->me_codes};
+                    h->me_codes, h->order};
     for (void* p : ptrs)
         if (p) cudaFree(p);
-    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
-    if (h->ev_join) cudaEventDestroy(h->ev_join);
-    if (h->side) cudaStreamDestroy(h->side);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return LBM_OK;
@@ -780,6 +798,7 @@ int lbm_step(lbm_lattice* h, int32_t n_steps)
         if (k > 0) {
             LaunchArgs a;
             a.P = h->P;
+            a.P.order = h->order;
             a.src = h->buf[h->cur];
             a.dst = h->buf[h->cur ^ 1];
             a.block = 256;
@@ -848,9 +867,7 @@ int lbm_step_planes(lbm_lattice* h, int32_t x_begin, int32_t x_end)
     a.tma_grid = 0;
     a.rule_quads = h->rule_quads;
     for (int k = 0; k < QUAD_KINDS; ++k) a.rule_counts[k] = h->rule_counts[k];
-    a.side = h->side;
-    a.fork = h->ev_fork;
-    a.join = h->ev_join;
+    a.rules_grid = h->rules_grid;
     cudaError_t e = h->storage == LBM_STORAGE_F64 ? launch_exact(KERNEL_STEP, h->desc.force_mode, a)
                                                   : launch_fast(h->storage, KERNEL_STEP, h->desc.force_mode, a);
     if (e != cudaSuccess) return cuda_fail(e, "plane-range step launch");

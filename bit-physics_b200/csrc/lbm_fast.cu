@@ -32,6 +32,35 @@ __global__ void k_list_rule_quads(Params P, int* __restrict__ lists, int cap, in
     lists[(size_t)kind * cap + atomicAdd(counts + kind, 1)] = q;
 }
 
+__global__ void k_face_order(Params P, int vec, int* __restrict__ order, int* __restrict__ face_count)
+{
+    const int nzi = P.nz / vec;  // items per row
+    const int items = P.n / vec;
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= items) return;
+    int x, y, z0;
+    decode_xyz(P, p * vec, x, y, z0);
+    const int zi = z0 / vec;
+    const int xo = P.walled[0] ? 1 : 0, yo = P.walled[1] ? 1 : 0, zo = P.walled[2] ? 1 : 0;
+    const int bx = P.nx - 2 * xo, by = P.ny - 2 * yo, bz = nzi - 2 * zo;
+    const bool inner = bx > 0 && by > 0 && bz > 0 && x >= xo && x < P.nx - xo && y >= yo && y < P.ny - yo &&
+                       zi >= zo && zi < nzi - zo;
+    if (inner) {
+        order[((x - xo) * by + (y - yo)) * bz + (zi - zo)] = p;
+    } else {
+        const int n_inner = bx > 0 && by > 0 && bz > 0 ? bx * by * bz : 0;
+        order[n_inner + atomicAdd(face_count, 1)] = p;
+    }
+}
+
+cudaError_t launch_face_order(const Params& P, int vec, int* order, int* face_count, cudaStream_t s)
+{
+    cudaError_t e = cudaMemsetAsync(face_count, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    k_face_order<<<grid_for(P.n / vec, 256), 256, 0, s>>>(P, vec, order, face_count);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_list_rule_quads(const Params& P, int* lists, int cap, int* counts, cudaStream_t s)
 {
     cudaError_t e = cudaMemsetAsync(counts, 0, sizeof(int) * QUAD_KINDS, s);
@@ -40,31 +69,23 @@ cudaError_t launch_list_rule_quads(const Params& P, int* lists, int cap, int* co
     return cudaGetLastError();
 }
 
-// k_step4 on the launch stream and, when the lattice has rule quads,
-// k_step4_rules on the side stream between a fork and a join event (the two
-// write disjoint cells and only read the source buffer).
+// k_step4 over the window's quads, led by the blocks that step the rule quads
+// (a.rules_grid of them, at most one task per thread).
 template <class M, int FM>
 static cudaError_t launch_step4(const LaunchArgs& a, const Streams<typename M::T>& S)
 {
-    cudaError_t e = cudaSuccess;
     const int total = a.rule_counts[0] + a.rule_counts[1] + a.rule_counts[2];
-    if (total > 0) {
-        if ((e = cudaEventRecord(a.fork, a.stream)) != cudaSuccess) return e;
-        if ((e = cudaStreamWaitEvent(a.side, a.fork, 0)) != cudaSuccess) return e;
-        const int* L = a.rule_quads;
-        const size_t cap = (size_t)a.P.n / 4;
-        const int rgrid = a.rules_grid > 0 ? a.rules_grid : grid_for(2LL * total, 128);
-        k_step4_rules<M, FM><<<rgrid, 128, 0, a.side>>>(
-            a.P, S, L + QUAD_KIND_NEAR * cap, L + QUAD_KIND_OUTFLOW * cap, L + QUAD_KIND_OTHER * cap,
-            a.rule_counts[QUAD_KIND_NEAR], a.rule_counts[QUAD_KIND_OUTFLOW], a.rule_counts[QUAD_KIND_OTHER]);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        if ((e = cudaEventRecord(a.join, a.side)) != cudaSuccess) return e;
-    }
+    const size_t cap = (size_t)a.P.n / 4;
+    const int* L = a.rule_quads;
+    RuleQuads rq{L + QUAD_KIND_NEAR * cap, L + QUAD_KIND_OUTFLOW * cap, L + QUAD_KIND_OTHER * cap,
+                 a.rule_counts[QUAD_KIND_NEAR], a.rule_counts[QUAD_KIND_OUTFLOW], a.rule_counts[QUAD_KIND_OTHER], 0};
     const int block = a.block < 128 ? a.block : 128;  // the kernel's bound
-    k_step4<M, FM><<<grid_for(window_cells(a.P) / 4, block), block, 0, a.stream>>>(a.P, S);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if (total > 0) e = cudaStreamWaitEvent(a.stream, a.join, 0);
-    return e;
+    if (total > 0) {
+        const int one_each = grid_for(2LL * total, block);
+        rq.blocks = a.rules_grid > 0 && a.rules_grid < one_each ? a.rules_grid : one_each;
+    }
+    k_step4<M, FM><<<rq.blocks + grid_for(window_cells(a.P) / 4, block), block, 0, a.stream>>>(a.P, S, rq);
+    return cudaGetLastError();
 }
 
 template <class M, int FM, int OUT>

@@ -50,11 +50,12 @@ struct lbm_lattice {
     int pipe_grid = 0;  // > 0: steps without outputs run k_step2_pipe
     int sums_grid = 0;  // > 0: steps with FP64 sums run k_step2_sums
     // Four-cell steps (vec == 4): the quads that need a boundary rule, stepped
-    // by k_step4_rules on a second stream beside k_step4.
+    // by the leading rules_grid blocks of k_step4.
     int* rule_quads = nullptr;  // QUAD_KINDS lists of n / 4 entries, then the counts
+    int* order = nullptr;       // Params::order of the plain one- / two-cell steps (walled lattices)
     int rule_counts[lbm::QUAD_KINDS] = {0, 0, 0};
-    cudaStream_t side = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    int rules_grid = 0;
+    int sms = 148;              // SMs of the lattice's device
     // Many steps per cooperative launch (LBM_STAGING_PERSISTENT): barrier
     // state, the limit of one barrier wait, and arrivals added to the
     // expected count (nonzero only through lbm_test_barrier_limit).

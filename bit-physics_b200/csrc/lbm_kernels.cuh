@@ -184,9 +184,14 @@ template <class M, int FM, int OUT>
 __global__ void __launch_bounds__(256, 3) k_step(Params P, Streams<typename M::T> S, Outputs<typename M::C> out)
 {
     if constexpr ((OUT & OUT_SUMS) != 0) reduce_prev(out);
-    const int idx = P.cell0 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = P.cell0 + blockIdx.x * blockDim.x + threadIdx.x;
     double cons[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    if (idx < P.n && idx < P.cell_end) step_single<M, FM, OUT>(P, S, out, idx, cons);
+    if (t < P.n && t < P.cell_end) {
+        int idx = t;
+        if constexpr (OUT == OUT_NONE)
+            if (P.order) idx = __ldg(P.order + t);
+        step_single<M, FM, OUT>(P, S, out, idx, cons);
+    }
     if constexpr ((OUT & OUT_SUMS) != 0) block_sum5(cons, out.partials + (size_t)blockIdx.x * 5);
 }
 
@@ -412,7 +417,8 @@ __global__ void __launch_bounds__(Step2Bounds<typename M::T>::threads, Step2Boun
         step_pair<M, FM, OUT>(P, S, out, live ? idx0 : P.n - 2, cons, live);
         block_sum5(cons, out.partials + (size_t)blockIdx.x * 5);
     } else {
-        if (idx0 < P.n && idx0 < P.cell_end) step_pair<M, FM, OUT>(P, S, out, idx0, cons);
+        if (idx0 < P.n && idx0 < P.cell_end)
+            step_pair<M, FM, OUT>(P, S, out, P.order ? 2 * __ldg(P.order + (idx0 >> 1)) : idx0, cons);
     }
 }
 
@@ -578,7 +584,7 @@ __device__ __forceinline__ uint32_t pack_dev2(float a, float b, __nv_bfloat16)
 // and none lies on a walled face: its post-stream state is the raw gather.
 // k_step4 also steps the quads of four solid cells (the rest state) and of
 // four inflow cells (feq(inflow) in every cell) off the walled faces; the
-// other quads are rule quads, listed by kind for k_step4_rules:
+// other quads are rule quads, listed by kind for k_step4's leading blocks:
 //   QUAD_KIND_NEAR     fluid and solid cells only, off the walled faces: one
 //                      round of loads (gather, cell words and the pair's own
 //                      slots, the half-way bounce-back sources) per pair;
@@ -595,78 +601,17 @@ __device__ __forceinline__ bool quad_on_walled_face(const Params& P, int x, int 
     return on_walled_face(P, x, y, z0) || on_walled_face(P, x, y, z0 + 3);
 }
 
-// Fused step from POST of the plain quads, four cells per thread, 16-bit
-// storage, nz a multiple of 4: the default step kernel of the 16-bit storages
-// when no readback or sums are asked for.  Every direction is one aligned
-// 8-byte load of the four cells' sources, plus one 2-byte load of the fifth
-// value a z-shifted direction needs; the packed collision runs on cells
-// (z0, z0 + 1), then (z0 + 2, z0 + 3), and each direction leaves as one
-// 8-byte store.  Against the two-cell kernel a thread keeps twice the bytes in
-// flight per load phase and issues fewer instructions per cell: 78.6 against
-// 66.0 GLUPS (f16) on the 256x128x128 lattice without flags, the same results
-// bit for bit.  The quads that need a rule (3.7 % of the sphere channel's)
-// return here and are stepped by k_step4_rules, launched beside this kernel
-// on a second stream: inside this kernel they would hold up their whole
-// warp (the rule quads sit in 23 % of the channel's rows), and their code
-// would raise the register demand of the plain path.  The flag bytes of the
-// quad are one 4-byte load issued with the gather.
-template <class M, int FM>
-__global__ void __launch_bounds__(128, 4) k_step4(Params P, Streams<typename M::T> S)
-{
-    using T = typename M::T;
-    static_assert(sizeof(T) == 2, "k_step4: 16-bit storage only");
-    const int idx0 = P.cell0 + 4 * (blockIdx.x * blockDim.x + threadIdx.x);
-    if (idx0 >= P.n || idx0 >= P.cell_end) return;
-    int x, y, z0;
-    decode_xyz(P, idx0, x, y, z0);
-    const Nbr nb0 = make_nbr(P, x, y, z0);
-    const int zr = z0 + 4 == P.nz ? 0 : z0 + 4;
-    uint2 raw[Q];
-    uint32_t edge[Q];
-#pragma unroll
-    for (int d = 0; d < Q; ++d) {
-        const unsigned short* p =
-            reinterpret_cast<const unsigned short*>(S.src[d]) + nb0.X[1 - cx(d)] + nb0.Y[1 - cy(d)];
-        raw[d] = __ldg(reinterpret_cast<const uint2*>(p + z0));
-        edge[d] = cz(d) == 1 ? (uint32_t)__ldg(p + nb0.Z[0]) : (cz(d) == -1 ? (uint32_t)__ldg(p + zr) : 0u);
-    }
-    const uint32_t fl4 = P.has_flags ? __ldg(reinterpret_cast<const uint32_t*>(P.flags + idx0)) : 0u;
-    if (fl4 != 0u || quad_on_walled_face(P, x, y, z0)) {
-        if (fl4 != QUAD_SOLID && fl4 != QUAD_INFLOW) return;  // a rule quad: k_step4_rules
-        if (quad_on_walled_face(P, x, y, z0)) return;
-        if (fl4 == QUAD_SOLID) {  // four solid cells: the rest state
-#pragma unroll
-            for (int d = 0; d < Q; ++d) {
-                const float2 sv = M::shift2(P, d, make_float2(0.0f, 0.0f));
-                const uint32_t w = pack_dev2(sv.x, sv.y, T{});
-                *reinterpret_cast<uint2*>(S.dst[d] + idx0) = make_uint2(w, w);
-            }
-            return;
-        }
-    }
-    const bool inflow4 = fl4 == QUAD_INFLOW;  // four inflow cells: feq(inflow) in every cell
-    uint32_t lo[Q];  // stored words of cells z0, z0 + 1
-#pragma unroll
-    for (int half = 0; half < 2; ++half) {
-        float2 h[Q];
-#pragma unroll
-        for (int d = 0; d < Q; ++d) {
-            uint32_t w;
-            if (cz(d) == 0) w = half == 0 ? raw[d].x : raw[d].y;
-            else if (cz(d) == 1) w = half == 0 ? (raw[d].x << 16) | edge[d] : __funnelshift_r(raw[d].x, raw[d].y, 16);
-            else w = half == 0 ? __funnelshift_r(raw[d].x, raw[d].y, 16) : __funnelshift_r(raw[d].y, edge[d], 16);
-            h[d] = inflow4 ? make_float2(P.inflow_h[d], P.inflow_h[d]) : M::unshift2(P, d, word_dev2(w, T{}));
-        }
-        M::template collide2<FM>(P, idx0 + 2 * half, h, [&](int d, float2 v) {
-            const float2 sv = M::shift2(P, d, v);
-            const uint32_t w = pack_dev2(sv.x, sv.y, T{});
-            if (half == 0) lo[d] = w;
-            else *reinterpret_cast<uint2*>(S.dst[d] + idx0) = make_uint2(lo[d], w);
-        });
-    }
-}
+// The rule quads of a k_step4 launch: quad lists by kind and the number of
+// leading blocks that step them.
+struct RuleQuads {
+    const int* near_q;
+    const int* out_q;
+    const int* other_q;
+    int n_near, n_out, n_other;
+    int blocks;
+};
 
-// One rule-quad pair task of k_step4_rules: tasks [0, 2 n_near) take the
+// One rule-quad pair task of k_step4: tasks [0, 2 n_near) take the
 // NEAR list, then the OUTFLOW list, then the OTHER list.
 template <class M, int FM>
 __device__ __forceinline__ void rule_pair(const Params& P, const Streams<typename M::T>& S, const int* near_q,
@@ -721,20 +666,93 @@ __device__ __forceinline__ void rule_pair(const Params& P, const Streams<typenam
     step_pair<M, FM, OUT_NONE>(P, S, none, idx0, nullptr);
 }
 
-// The rule quads of k_step4 in a grid-stride loop over the pair tasks.  The
-// launch gives it a small grid: it runs beside k_step4 on a few SMs, its
-// latency-bound tasks spread over k_step4's run, instead of filling every SM
-// for a short while and holding k_step4's blocks back.
+// Fused step from POST of the plain quads, four cells per thread, 16-bit
+// storage, nz a multiple of 4: the default step kernel of the 16-bit storages
+// when no readback or sums are asked for.  Every direction is one aligned
+// 8-byte load of the four cells' sources, plus one 2-byte load of the fifth
+// value a z-shifted direction needs; the packed collision runs on cells
+// (z0, z0 + 1), then (z0 + 2, z0 + 3), and each direction leaves as one
+// 8-byte store.  Against the two-cell kernel a thread keeps twice the bytes in
+// flight per load phase and issues fewer instructions per cell: 78.6 against
+// 66.0 GLUPS (f16) on the 256x128x128 lattice without flags, the same results
+// bit for bit.  The quads that need a rule (3.7 % of the sphere channel's)
+// return from the plain path: there they would hold up their whole warp (the
+// rule quads sit in 23 % of the channel's rows), and their code would raise
+// the register demand of the plain path.  The first `rblocks` blocks of the
+// launch step them instead, in a grid-stride loop over their pair tasks
+// (rule_pair): the block scheduler starts those blocks first, and they run on
+// a few SMs beside the plain blocks for the whole launch.  On the sphere
+// channel (23,930 rule quads, f16) 32 such blocks take the launch from 66.5
+// (the rule quads as a second kernel on a second stream) to 60.1 us, against
+// 58.0 us for the plain quads alone.  The flag bytes of the quad are one
+// 4-byte load issued with the gather.
 template <class M, int FM>
-__global__ void __launch_bounds__(128) k_step4_rules(Params P, Streams<typename M::T> S, const int* __restrict__ near_q,
-                                                     const int* __restrict__ out_q, const int* __restrict__ other_q,
-                                                     int n_near, int n_out, int n_other)
+__global__ void __launch_bounds__(128, 4) k_step4(Params P, Streams<typename M::T> S, RuleQuads rq)
 {
-    const int total = 2 * (n_near + n_out + n_other);
+    using T = typename M::T;
+    static_assert(sizeof(T) == 2, "k_step4: 16-bit storage only");
+    if ((int)blockIdx.x < rq.blocks) {
+        const int total = 2 * (rq.n_near + rq.n_out + rq.n_other);
 #pragma unroll 1
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x)
-        rule_pair<M, FM>(P, S, near_q, out_q, other_q, n_near, n_out, n_other, k);
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += rq.blocks * blockDim.x)
+            rule_pair<M, FM>(P, S, rq.near_q, rq.out_q, rq.other_q, rq.n_near, rq.n_out, rq.n_other, k);
+        return;
+    }
+    const int idx0 = P.cell0 + 4 * ((blockIdx.x - rq.blocks) * blockDim.x + threadIdx.x);
+    if (idx0 >= P.n || idx0 >= P.cell_end) return;
+    int x, y, z0;
+    decode_xyz(P, idx0, x, y, z0);
+    const Nbr nb0 = make_nbr(P, x, y, z0);
+    const int zr = z0 + 4 == P.nz ? 0 : z0 + 4;
+    uint2 raw[Q];
+    uint32_t edge[Q];
+#pragma unroll
+    for (int d = 0; d < Q; ++d) {
+        const unsigned short* p =
+            reinterpret_cast<const unsigned short*>(S.src[d]) + nb0.X[1 - cx(d)] + nb0.Y[1 - cy(d)];
+        raw[d] = __ldg(reinterpret_cast<const uint2*>(p + z0));
+        edge[d] = cz(d) == 1 ? (uint32_t)__ldg(p + nb0.Z[0]) : (cz(d) == -1 ? (uint32_t)__ldg(p + zr) : 0u);
+    }
+    const uint32_t fl4 = P.has_flags ? __ldg(reinterpret_cast<const uint32_t*>(P.flags + idx0)) : 0u;
+    if (fl4 != 0u || quad_on_walled_face(P, x, y, z0)) {
+        if (fl4 != QUAD_SOLID && fl4 != QUAD_INFLOW) return;  // a rule quad: the leading blocks
+        if (quad_on_walled_face(P, x, y, z0)) return;
+        if (fl4 == QUAD_SOLID) {  // four solid cells: the rest state
+#pragma unroll
+            for (int d = 0; d < Q; ++d) {
+                const float2 sv = M::shift2(P, d, make_float2(0.0f, 0.0f));
+                const uint32_t w = pack_dev2(sv.x, sv.y, T{});
+                *reinterpret_cast<uint2*>(S.dst[d] + idx0) = make_uint2(w, w);
+            }
+            return;
+        }
+    }
+    const bool inflow4 = fl4 == QUAD_INFLOW;  // four inflow cells: feq(inflow) in every cell
+    uint32_t lo[Q];  // stored words of cells z0, z0 + 1
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+        float2 h[Q];
+#pragma unroll
+        for (int d = 0; d < Q; ++d) {
+            uint32_t w;
+            if (cz(d) == 0) w = half == 0 ? raw[d].x : raw[d].y;
+            else if (cz(d) == 1) w = half == 0 ? (raw[d].x << 16) | edge[d] : __funnelshift_r(raw[d].x, raw[d].y, 16);
+            else w = half == 0 ? __funnelshift_r(raw[d].x, raw[d].y, 16) : __funnelshift_r(raw[d].y, edge[d], 16);
+            h[d] = inflow4 ? make_float2(P.inflow_h[d], P.inflow_h[d]) : M::unshift2(P, d, word_dev2(w, T{}));
+        }
+        M::template collide2<FM>(P, idx0 + 2 * half, h, [&](int d, float2 v) {
+            const float2 sv = M::shift2(P, d, v);
+            const uint32_t w = pack_dev2(sv.x, sv.y, T{});
+            if (half == 0) lo[d] = w;
+            else *reinterpret_cast<uint2*>(S.dst[d] + idx0) = make_uint2(lo[d], w);
+        });
+    }
 }
+
+// The visit order of Params::order for items of `vec` cells (1 or 2): the
+// items off the walled faces at their rank in the interior box, the others
+// appended after them through *face_count.
+__global__ void k_face_order(Params P, int vec, int* __restrict__ order, int* __restrict__ face_count);
 
 // Lists of the rule quads by kind: quad indices of kind k at lists + k * cap,
 // their number in counts[k] (order unspecified; each quad's work is
@@ -818,8 +836,9 @@ __global__ void __launch_bounds__(256) k_step_persistent(Params P, Streams<typen
     for (int s = 0; s < steps; ++s) {
         const Streams<typename M::T>& S = (s & 1) ? S1 : S0;
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < items; i += gridDim.x * blockDim.x) {
-            if constexpr (VEC == 2) step_pair<M, FM, OUT_NONE>(P, S, none, 2 * i, nullptr);
-            else step_single<M, FM, OUT_NONE>(P, S, none, i, nullptr);
+            const int it = P.order ? __ldg(P.order + i) : i;
+            if constexpr (VEC == 2) step_pair<M, FM, OUT_NONE>(P, S, none, 2 * it, nullptr);
+            else step_single<M, FM, OUT_NONE>(P, S, none, it, nullptr);
         }
         if (s + 1 < steps && !grid_sync(bar, P.err, expected, timeout_ns)) return;
     }

@@ -37,13 +37,11 @@ struct LaunchArgs {
                         // k_step2_pipe with this grid
     int sums_grid = 0;  // > 0: a two-cell KERNEL_STEP with partials runs
                         // k_step2_sums with this grid
-    // vec == 4 steps without outputs: the rule quads (k_step4_rules) run on
-    // `side` between the fork and join events
+    // vec == 4 steps without outputs: the rule quads, stepped by k_step4's
+    // leading blocks
     const int* rule_quads = nullptr;  // QUAD_KINDS lists of n / 4 entries
     int rule_counts[QUAD_KINDS] = {0, 0, 0};
-    int rules_grid = 0;  // blocks of k_step4_rules (0: one task per thread)
-    cudaStream_t side = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr;
+    int rules_grid = 0;  // leading blocks (0: one task per thread)
 };
 
 // Output selection of a step launch (OUT_* bits of lbm_kernels.cuh) from the
@@ -70,6 +68,9 @@ cudaError_t launch_mark_near_solid(const Params& P, uint8_t* flags, uint32_t* bb
 // k_step4_rules, by kind into lists + kind * cap; their numbers into
 // counts[QUAD_KINDS] (device).
 cudaError_t launch_list_rule_quads(const Params& P, int* lists, int cap, int* counts, cudaStream_t s);
+// Params::order for items of vec (1 or 2) cells; *face_count (device)
+// receives the number of items on the walled faces.
+cudaError_t launch_face_order(const Params& P, int vec, int* order, int* face_count, cudaStream_t s);
 cudaError_t launch_reduce_partials(const double* partials, int nblocks, double* out5, cudaStream_t s);
 // Tier-1 / Tier-2 diagnostics of f64 rho (n) / u (3, n) device arrays into
 // out6 (device): {check_health, rho_min, rho_max, u_max_lat,

@@ -1,5 +1,5 @@
-"""The four-cell 16-bit step (k_step4 for the plain quads, k_step4_rules on a
-second stream for the quads that need a boundary rule) on a B200.
+"""The four-cell 16-bit step (k_step4: the plain quads, and in its leading
+blocks the quads that need a boundary rule) on a B200.
 
 Lattices with many solid cells, walled faces, inflow / outflow planes and
 per-cell forces, stepped with the one-, two- and four-cell kernels mixed with
