@@ -489,8 +489,8 @@ int lbm_create(const lbm_desc* desc, lbm_lattice** out)
     rebuild_params(h);
     if (int rc2 = refresh_rule_quads(h)) return cleanup(rc2);
     // Visit order of the plain one- and two-cell steps on a lattice with
-    // walls: interior items first, then those on the walled faces (fixed by
-    // the periodicity, which does not change after creation).
+    // walls: the items on the walled faces first, then the interior (fixed
+    // by the periodicity, which does not change after creation).
     if (h->vec <= 2 && desc->periodic != 7) {
         const size_t items = (size_t)h->n / h->vec;
         e = cudaMalloc((void**)&h->order, sizeof(int) * (items + 1));

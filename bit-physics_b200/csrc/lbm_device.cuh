@@ -114,9 +114,10 @@ struct Params {
     // quads, k_collide_local): they advance the cells [cell0, min(n, cell_end)).
     int cell0 = 0, cell_end = 0x7fffffff;
     // Visit order of the plain steps of k_step (cells), k_step2 (pairs) and
-    // k_step_persistent: item t is order[t], the items off the walled faces
-    // first, then those on them, so that a warp runs one of the two paths
-    // (results do not depend on the order).  Null: item t is t.
+    // k_step_persistent: item t is order[t], the items on the walled faces
+    // first (the slower ones start first), then the others, so that a warp
+    // runs one of the two paths (results do not depend on the order).  Null:
+    // item t is t.
     const int* order = nullptr;
 };
 

@@ -45,12 +45,11 @@ __global__ void k_face_order(Params P, int vec, int* __restrict__ order, int* __
     const int bx = P.nx - 2 * xo, by = P.ny - 2 * yo, bz = nzi - 2 * zo;
     const bool inner = bx > 0 && by > 0 && bz > 0 && x >= xo && x < P.nx - xo && y >= yo && y < P.ny - yo &&
                        zi >= zo && zi < nzi - zo;
-    if (inner) {
-        order[((x - xo) * by + (y - yo)) * bz + (zi - zo)] = p;
-    } else {
-        const int n_inner = bx > 0 && by > 0 && bz > 0 ? bx * by * bz : 0;
-        order[n_inner + atomicAdd(face_count, 1)] = p;
-    }
+    const int n_inner = bx > 0 && by > 0 && bz > 0 ? bx * by * bz : 0;
+    if (inner)
+        order[items - n_inner + ((x - xo) * by + (y - yo)) * bz + (zi - zo)] = p;
+    else
+        order[atomicAdd(face_count, 1)] = p;
 }
 
 cudaError_t launch_face_order(const Params& P, int vec, int* order, int* face_count, cudaStream_t s)

@@ -750,8 +750,8 @@ __global__ void __launch_bounds__(128, 4) k_step4(Params P, Streams<typename M::
 }
 
 // The visit order of Params::order for items of `vec` cells (1 or 2): the
-// items off the walled faces at their rank in the interior box, the others
-// appended after them through *face_count.
+// items on the walled faces first (appended through *face_count), then the
+// others at their rank in the interior box.
 __global__ void k_face_order(Params P, int vec, int* __restrict__ order, int* __restrict__ face_count);
 
 // Lists of the rule quads by kind: quad indices of kind k at lists + k * cap,

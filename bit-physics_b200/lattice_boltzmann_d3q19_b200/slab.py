@@ -254,6 +254,28 @@ def step_distributed(slab: SlabLattice, rank: int, world: int, comm_stream=None,
     slab.step_boundary()
 
 
+def conservation_distributed(slab: SlabLattice, rank: int, world: int, to_tensor=None,
+                             from_tensor=None) -> np.ndarray:
+    """FP64 {mass, momentum x, y, z} of the whole lattice: each rank's sums
+    over its owned planes (after a face exchange, which the readback of a
+    boundary plane pulls from; to_tensor / from_tensor as for
+    exchange_distributed), added by an all-reduce of 4 doubles (NCCL on the
+    engine's device for a GpuEngine, gloo on the host otherwise)."""
+    import torch
+    import torch.distributed as dist
+
+    if slab.stepped:
+        exchange_distributed(slab, rank, world, to_tensor, from_tensor)
+    local = np.asarray(slab.engine.conservation_planes(1, slab.width + 1), dtype=np.float64)
+    if world == 1:
+        return local
+    like = getattr(slab.engine, "send", (None,))[0]
+    dev = like.device if like is not None and getattr(like, "is_cuda", False) else torch.device("cpu")
+    t = torch.tensor(local, dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return t.cpu().numpy()
+
+
 class GpuEngine:
     """Adapter of a Lattice (local slab shape) to the SlabLattice engine
     interface: plane buffers are torch device tensors, allocated once (two
@@ -305,4 +327,4 @@ class GpuEngine:
 
 
 __all__ = ["GpuEngine", "MASK_MINUS", "MASK_PLUS", "MINUS_X", "PLUS_X", "SlabGroup", "SlabLattice",
-           "exchange_distributed", "slab_bounds", "step_distributed", "with_halos"]
+           "conservation_distributed", "exchange_distributed", "slab_bounds", "step_distributed", "with_halos"]

@@ -15,7 +15,8 @@ import torch.multiprocessing as mp
 from adjoint_cases import case, oracle_lattice
 from slab_cases import oracle_slab
 
-from lattice_boltzmann_d3q19_b200.slab import SlabGroup, exchange_distributed, slab_bounds, step_distributed, with_halos
+from lattice_boltzmann_d3q19_b200.slab import SlabGroup, conservation_distributed, exchange_distributed, slab_bounds, \
+    step_distributed, with_halos
 
 
 def test_slab_bounds_and_halos():
@@ -81,7 +82,8 @@ def _rank_main(rank, world, port, n_steps, out_dir, split):
             s.engine.step(1)
         exchange_distributed(s, rank, world, to_t, from_t)
         rho, u = s.engine.rho_u()
-        np.savez(os.path.join(out_dir, f"rank{rank}.npz"), rho=s.owned(rho, 0), u=s.owned(u, 1))
+        cons = conservation_distributed(s, rank, world, to_t, from_t)
+        np.savez(os.path.join(out_dir, f"rank{rank}.npz"), rho=s.owned(rho, 0), u=s.owned(u, 1), cons=cons)
     finally:
         dist.destroy_process_group()
 
@@ -111,3 +113,6 @@ def test_two_gloo_ranks_match_unsplit(tmp_path, split):
     ref.step(n_steps)
     rho_ref, u_ref = ref.rho_u()
     assert np.array_equal(rho, rho_ref) and np.array_equal(u, u_ref)
+    # the all-reduced FP64 sums: the same on both ranks, those of the whole lattice
+    assert np.array_equal(parts[0]["cons"], parts[1]["cons"])
+    np.testing.assert_allclose(parts[0]["cons"], ref.conservation(), rtol=1e-13, atol=1e-13)
