@@ -213,12 +213,14 @@ int refresh_rule_quads(lbm_lattice* h)
     CK(cudaMemcpyAsync(h->rule_counts, counts, sizeof(int) * QUAD_KINDS, cudaMemcpyDeviceToHost, h->stream),
        "rule quad counts");
     CK(cudaStreamSynchronize(h->stream), "rule quad sync");
-    // Leading blocks of k_step4: about as many rule tasks per thread as the
-    // plain quads take waves of resident blocks (4 of 128 threads per SM),
-    // so that the rule blocks finish with the plain ones.
+    // Leading blocks of k_step4: about 0.8 rule tasks per thread for each
+    // wave of resident blocks (4 of 128 threads per SM) the plain quads take,
+    // so that the rule blocks finish within the plain ones' time.  Sphere
+    // channel (23,930 rule quads): 35 blocks; measured 59.0 us at 32 and
+    // 59.5 at 36 (the plain quads alone: 59.3), 61.5 at 28, 66.1 at 24.
     const long long total = (long long)h->rule_counts[0] + h->rule_counts[1] + h->rule_counts[2];
     const long long plain = (long long)cap - total > 0 ? (long long)cap - total : 1;
-    const long long want = (2 * total * 4 * h->sms + plain - 1) / plain;
+    const long long want = (2 * total * 5 * h->sms + plain - 1) / plain;
     h->rules_grid = total > 0 ? (int)(want < 1 ? 1 : (want > 4 * h->sms ? 4 * h->sms : want)) : 0;
     h->params_version += 1;  // a captured step graph holds the old count
     return LBM_OK;
@@ -798,7 +800,6 @@ int lbm_step(lbm_lattice* h, int32_t n_steps)
         if (k > 0) {
             LaunchArgs a;
             a.P = h->P;
-            a.P.order = h->order;
             a.src = h->buf[h->cur];
             a.dst = h->buf[h->cur ^ 1];
             a.block = 256;

@@ -113,11 +113,13 @@ struct Params {
     // Cell window of the step kernels (k_step, k_step2, k_step4 with its rule
     // quads, k_collide_local): they advance the cells [cell0, min(n, cell_end)).
     int cell0 = 0, cell_end = 0x7fffffff;
-    // Visit order of the plain steps of k_step (cells), k_step2 (pairs) and
-    // k_step_persistent: item t is order[t], the items on the walled faces
-    // first (the slower ones start first), then the others, so that a warp
-    // runs one of the two paths (results do not depend on the order).  Null:
-    // item t is t.
+    // Visit order of the plain steps of k_step (cells) and k_step2 (pairs):
+    // item t is order[t], the items on the walled faces first (the slower
+    // ones start first), then the others, so that a warp runs one of the
+    // two paths (results do not depend on the order).  Null: item t is t.
+    // (The persistent kernel deals items to its blocks statically: there
+    // the face items gathered into a few blocks would set each step's time,
+    // so it keeps them spread.)
     const int* order = nullptr;
 };
 

@@ -836,9 +836,8 @@ __global__ void __launch_bounds__(256) k_step_persistent(Params P, Streams<typen
     for (int s = 0; s < steps; ++s) {
         const Streams<typename M::T>& S = (s & 1) ? S1 : S0;
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < items; i += gridDim.x * blockDim.x) {
-            const int it = P.order ? __ldg(P.order + i) : i;
-            if constexpr (VEC == 2) step_pair<M, FM, OUT_NONE>(P, S, none, 2 * it, nullptr);
-            else step_single<M, FM, OUT_NONE>(P, S, none, it, nullptr);
+            if constexpr (VEC == 2) step_pair<M, FM, OUT_NONE>(P, S, none, 2 * i, nullptr);
+            else step_single<M, FM, OUT_NONE>(P, S, none, i, nullptr);
         }
         if (s + 1 < steps && !grid_sync(bar, P.err, expected, timeout_ns)) return;
     }

@@ -134,12 +134,14 @@ def test_c1_cavity_proxy_reduced_storage_1000_steps(storage, c1_reference):
 
 # 5000 steps of the headline channel: u error over fluid cells, L2 of the
 # error field relative to the L2 of the f64 field, and the largest error
-# magnitude relative to the largest f64 speed.  Bounds: (L2-rel, max-rel),
-# about twice the values measured on a B200 (f32 1.1e-4 / 8.4e-4 at tau
-# 0.51; f16 3.4e-3 / 9.4e-3 at tau 0.8; bf16 2.2e-2 / 1.2e-1).
+# magnitude relative to the largest f64 speed.  Bounds: (L2-rel, max-rel).
+# The 16-bit storages hold deviations from feq(1, inflow velocity); f16 is
+# held to the 1e-3 L2-relative target at every tau (measured on a B200 at
+# 2000 steps: 1.1e-4, 5.4e-5, 1.2e-4 at tau 0.51 / 0.56 / 0.8).  f32 and
+# bf16: about twice the values measured.
 PRECISION_BOUND = {
     "f32": {0.51: (2.5e-4, 2e-3), 0.56: (5e-5, 1e-4), 0.8: (1.5e-4, 2e-4)},
-    "f16": {0.51: (1.2e-3, 5e-3), 0.56: (1.2e-3, 5e-3), 0.8: (7e-3, 2e-2)},
+    "f16": {0.51: (1e-3, 1e-2), 0.56: (1e-3, 1e-2), 0.8: (1e-3, 1e-2)},
     "bf16": {0.51: (2.5e-2, 2.5e-1), 0.56: (2.5e-2, 1e-1), 0.8: (4.5e-2, 1.3e-1)},
 }
 
