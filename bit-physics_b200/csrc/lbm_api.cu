@@ -159,6 +159,22 @@ void rebuild_params(lbm_lattice* h)
         const double feq = P.w[q] * 1.0 * (1.0 + cu * P.inv_cs2 + cu * cu * P.inv_two_cs4 - r_sq * P.inv_two_cs2);
         P.shift_h[q] = storage16 ? (float)(feq - P.w[q]) : 0.0f;
     }
+    // The shift's constants of ModeFast::collide2s (f32, as the kernels use them).
+    float sum = 0.0f, m[3] = {0.0f, 0.0f, 0.0f};
+    for (int q = 0; q < Q; ++q) {
+        sum += P.shift_h[q];
+        m[0] += (float)cx(q) * P.shift_h[q];
+        m[1] += (float)cy(q) * P.shift_h[q];
+        m[2] += (float)cz(q) * P.shift_h[q];
+        P.inflow_s[q] = P.inflow_h[q] - P.shift_h[q];
+    }
+    P.sh_sum = sum;
+    for (int a = 0; a < 3; ++a) P.sh_m[a] = m[a];
+    P.sh_c0 = -P.omega * P.shift_h[0];
+    for (int q = 1; q < Q; q += 2) {
+        P.sh_csym[q >> 1] = -P.omega * (0.5f * (P.shift_h[q] + P.shift_h[q + 1]));
+        P.sh_casym[q >> 1] = -P.omega * (0.5f * (P.shift_h[q] - P.shift_h[q + 1]));
+    }
 }
 
 }  // namespace

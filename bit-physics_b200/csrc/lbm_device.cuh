@@ -110,6 +110,14 @@ struct Params {
     // from feq_d(1, storage_ref_u), i.e. (f - w_d) - shift_h[d] in f32; zero
     // for the other storages.
     float shift_h[Q];
+    // The same shift folded into the collision of stored values s = h - shift
+    // (ModeFast::collide2s; zero for the other storages): its sum and first
+    // moments, the relaxation's constant terms -omega shift per direction as
+    // the (symmetric, antisymmetric) halves of each opposite pair, and the
+    // inflow state as stored values.
+    float sh_sum, sh_m[3];
+    float sh_c0, sh_csym[Q / 2], sh_casym[Q / 2];
+    float inflow_s[Q];
     // Cell window of the step kernels (k_step, k_step2, k_step4 with its rule
     // quads, k_collide_local): they advance the cells [cell0, min(n, cell_end)).
     int cell0 = 0, cell_end = 0x7fffffff;
@@ -622,6 +630,94 @@ struct ModeFast {
             sink(d + 1, h[d + 1]);
         }
         return {rd, mx, my, mz};
+    }
+
+    // collide2 on the stored values of a 16-bit storage (s = h - shift_h,
+    // as loaded; sink receives the post-collision stored values): the shift
+    // enters through constants instead of an add per value on the way in and
+    // out, since h_new - shift = (1 - omega) s + sym +- asym - omega shift.
+    // The same collision as collide2 in exact arithmetic; the f32 roundings
+    // differ (both far below the 16-bit rounding of the stored result).
+    template <int FM, class Sink>
+    static __device__ __forceinline__ void collide2s(const Params& P, int cell0, float2* s, Sink&& sink)
+    {
+        float2 rs = s[0];
+#pragma unroll
+        for (int d = 1; d < Q; ++d) rs = add2(rs, s[d]);
+        const float2 rd = add2(rs, bc2(P.sh_sum));
+        const float2 p1 = sub2(s[1], s[2]), p3 = sub2(s[3], s[4]), p5 = sub2(s[5], s[6]);
+        const float2 p7 = sub2(s[7], s[8]), p9 = sub2(s[9], s[10]), p11 = sub2(s[11], s[12]);
+        const float2 p13 = sub2(s[13], s[14]), p15 = sub2(s[15], s[16]), p17 = sub2(s[17], s[18]);
+        const float2 mx = add2(add2(add2(add2(p1, p7), add2(p9, p11)), p13), bc2(P.sh_m[0]));
+        const float2 my = add2(add2(add2(sub2(add2(p3, p7), p9), p15), p17), bc2(P.sh_m[1]));
+        const float2 mz = add2(sub2(add2(sub2(add2(p5, p11), p13), p15), p17), bc2(P.sh_m[2]));
+        const float2 rho = add2(rd, bc2(1.0f));
+        const float2 inv = make_float2(__fdividef(1.0f, rho_safe(rho.x)), __fdividef(1.0f, rho_safe(rho.y)));
+        float2 Fx = bc2(0.0f), Fy = bc2(0.0f), Fz = bc2(0.0f);
+        if constexpr (FM == FORCE_UNIFORM) {
+            Fx = bc2(P.body_force_f[0]); Fy = bc2(P.body_force_f[1]); Fz = bc2(P.body_force_f[2]);
+        } else if constexpr (FM == FORCE_FIELD) {
+            const float* F = (const float*)P.force;
+            Fx = __ldg(reinterpret_cast<const float2*>(F + cell0));
+            Fy = __ldg(reinterpret_cast<const float2*>(F + P.n + cell0));
+            Fz = __ldg(reinterpret_cast<const float2*>(F + 2 * P.n + cell0));
+        } else if constexpr (FM == FORCE_DRAG) {
+            const float2 a = __ldg(reinterpret_cast<const float2*>(P.porosity + cell0));
+            const float2 ka = mul2(bc2(P.drag_kf), a);
+            const float2 den = fma2(bc2(0.5f), ka, bc2(1.0f));
+            const float2 nbeta = make_float2(-__fdividef(ka.x, den.x), -__fdividef(ka.y, den.y));
+            Fx = fma2(nbeta, mx, bc2(P.body_force_f[0]));
+            Fy = fma2(nbeta, my, bc2(P.body_force_f[1]));
+            Fz = fma2(nbeta, mz, bc2(P.body_force_f[2]));
+        }
+        float2 ux, uy, uz;
+        if constexpr (FM == FORCE_NONE) {
+            ux = mul2(mx, inv); uy = mul2(my, inv); uz = mul2(mz, inv);
+        } else {
+            ux = mul2(fma2(bc2(0.5f), Fx, mx), inv);
+            uy = mul2(fma2(bc2(0.5f), Fy, my), inv);
+            uz = mul2(fma2(bc2(0.5f), Fz, mz), inv);
+        }
+        const float2 usq = fma2(uz, uz, fma2(uy, uy, mul2(ux, ux)));
+        const float2 base = fma2(rho, mul2(usq, bc2(-1.5f)), rd);  // rho_dev - 1.5 rho u^2
+        const float om = P.omega;
+        const float2 keep = bc2(1.0f - om);
+        const float2 rho45 = mul2(rho, bc2(4.5f));
+        const float2 asym18 = mul2(rho, bc2(3.0f * om * wf(1)));
+        const float2 asym36 = mul2(rho, bc2(3.0f * om * wf(7)));
+        float2 nuF3 = bc2(0.0f);
+        if constexpr (FM != FORCE_NONE) nuF3 = mul2(bc2(-3.0f), fma2(uz, Fz, fma2(uy, Fy, mul2(ux, Fx))));
+        s[0] = fma2(keep, s[0], fma2(bc2(om * wf(0)), base, bc2(P.sh_c0)));
+        if constexpr (FM != FORCE_NONE) s[0] = fma2(bc2(P.pref * wf(0)), nuF3, s[0]);
+        sink(0, s[0]);
+#pragma unroll
+        for (int d = 1; d < Q; d += 2) {
+            float2 cu, cF;
+            switch (d) {
+            case 1: cu = ux; cF = Fx; break;
+            case 3: cu = uy; cF = Fy; break;
+            case 5: cu = uz; cF = Fz; break;
+            case 7: cu = add2(ux, uy); cF = add2(Fx, Fy); break;
+            case 9: cu = sub2(ux, uy); cF = sub2(Fx, Fy); break;
+            case 11: cu = add2(ux, uz); cF = add2(Fx, Fz); break;
+            case 13: cu = sub2(ux, uz); cF = sub2(Fx, Fz); break;
+            case 15: cu = add2(uy, uz); cF = add2(Fy, Fz); break;
+            default: cu = sub2(uy, uz); cF = sub2(Fy, Fz); break;
+            }
+            const float w = wf(d);
+            const float2 s1 = fma2(mul2(rho45, cu), cu, base);
+            float2 sym = fma2(bc2(om * w), s1, bc2(P.sh_csym[d >> 1]));
+            float2 asym = fma2(d < 7 ? asym18 : asym36, cu, bc2(P.sh_casym[d >> 1]));
+            if constexpr (FM != FORCE_NONE) {
+                const float pw = P.pref * w;
+                sym = fma2(bc2(pw), fma2(mul2(bc2(9.0f), cu), cF, nuF3), sym);
+                asym = fma2(bc2(3.0f * pw), cF, asym);
+            }
+            s[d] = fma2(keep, s[d], add2(sym, asym));
+            s[d + 1] = fma2(keep, s[d + 1], sub2(sym, asym));
+            sink(d, s[d]);
+            sink(d + 1, s[d + 1]);
+        }
     }
 
     template <int FM>

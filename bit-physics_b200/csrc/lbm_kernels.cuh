@@ -738,11 +738,10 @@ __global__ void __launch_bounds__(128, 4) k_step4(Params P, Streams<typename M::
             if (cz(d) == 0) w = half == 0 ? raw[d].x : raw[d].y;
             else if (cz(d) == 1) w = half == 0 ? (raw[d].x << 16) | edge[d] : __funnelshift_r(raw[d].x, raw[d].y, 16);
             else w = half == 0 ? __funnelshift_r(raw[d].x, raw[d].y, 16) : __funnelshift_r(raw[d].y, edge[d], 16);
-            h[d] = inflow4 ? make_float2(P.inflow_h[d], P.inflow_h[d]) : M::unshift2(P, d, word_dev2(w, T{}));
+            h[d] = inflow4 ? make_float2(P.inflow_s[d], P.inflow_s[d]) : word_dev2(w, T{});
         }
-        M::template collide2<FM>(P, idx0 + 2 * half, h, [&](int d, float2 v) {
-            const float2 sv = M::shift2(P, d, v);
-            const uint32_t w = pack_dev2(sv.x, sv.y, T{});
+        M::template collide2s<FM>(P, idx0 + 2 * half, h, [&](int d, float2 v) {
+            const uint32_t w = pack_dev2(v.x, v.y, T{});
             if (half == 0) lo[d] = w;
             else *reinterpret_cast<uint2*>(S.dst[d] + idx0) = make_uint2(lo[d], w);
         });

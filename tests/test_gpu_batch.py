@@ -25,10 +25,16 @@ def _specs(storage, lids=(0.05, 0.03, 0.02, 0.07, 0.04), taus=(0.6, 0.55, 0.8, 0
 
 
 def _singles(specs, cells_per_thread):
+    """Single lattices of the specs; cells_per_thread "pairs": the two-cell
+    kernel where nz is even (the batch's pair schedules share its collision),
+    one cell per thread otherwise."""
     out = []
     for sp in specs:
         kw = dict(sp)
-        out.append(Lattice(kw.pop("shape"), kw.pop("tau"), cells_per_thread=cells_per_thread, **kw))
+        cpt = cells_per_thread
+        if cpt == "pairs":
+            cpt = 2 if kw["shape"][2] % 2 == 0 else 1
+        out.append(Lattice(kw.pop("shape"), kw.pop("tau"), cells_per_thread=cpt, **kw))
     return out
 
 
@@ -55,7 +61,7 @@ def test_f64_batch_bit_exact_with_oracle():
 def test_fast_batch_matches_single_lattices(storage, schedule):
     specs = _specs(storage)
     states = [random_state(sp["shape"], 60 + k, amp=0.01) for k, sp in enumerate(specs)]
-    cpt = 1 if schedule == "single" else 0
+    cpt = 1 if schedule == "single" else "pairs"
     singles = _singles(specs, cpt)
     with Batch(specs) as b:
         b.set_schedule(schedule, block=128, grid=37)

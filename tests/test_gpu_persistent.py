@@ -43,8 +43,14 @@ def test_persistent_matches_a_launch_per_step(storage):
     flags[-1] = 3
     f0 = random_state(shape, 8, amp=0.01)
     out = {}
-    for staging in ("auto", "persistent"):
-        with Lattice(shape, 0.58, storage=storage, staging=staging, inflow_u=(0.04, 0.0, 0.0),
+    # the persistent kernel steps pairs: against a launch per step of the
+    # two-cell kernel bit for bit, and of the default (16-bit: four-cell,
+    # shift folded into the collision constants) within tolerance
+    runs = [("auto", 0), ("persistent", 0)]
+    if storage in ("f16", "bf16"):
+        runs.append(("registers", 2))
+    for staging, cpt in runs:
+        with Lattice(shape, 0.58, storage=storage, staging=staging, cells_per_thread=cpt, inflow_u=(0.04, 0.0, 0.0),
                      periodic=(True, False, True), wall_velocity={"y+": (0.03, 0.0, 0.0)}) as lat:
             lat.set_flags(flags)
             lat.set_populations(f0)
@@ -53,7 +59,10 @@ def test_persistent_matches_a_launch_per_step(storage):
             lat.step(3)
             out[staging] = (lat.get_populations(), lat.step_count)
     assert out["auto"][1] == out["persistent"][1] == 44
-    assert same_bytes(out["auto"][0], out["persistent"][0])
+    same = out["registers" if storage in ("f16", "bf16") else "auto"][0]
+    assert same_bytes(same, out["persistent"][0])
+    tol = {"f64": 0.0, "f32": 0.0, "f16": 2e-4, "bf16": 2e-3}[storage]
+    assert float(np.max(np.abs(out["auto"][0] - out["persistent"][0]))) <= tol
 
 
 def test_barrier_that_never_opens_times_out_and_reports():
