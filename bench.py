@@ -238,7 +238,7 @@ def make_lattice(storage: str, flags, device: int):
 # ---------------------------------------------------------------------------
 # reference arm / CPU baseline: the f64 CPU oracle on a bounded sample
 # ---------------------------------------------------------------------------
-def cpu_reference_rate(flags, budget_s: float, max_steps: int):
+def cpu_reference_rate(flags, budget_s: float, max_steps: int, warmup: int = 1):
     import oracle as O
 
     threads = O.num_threads()
@@ -247,16 +247,18 @@ def cpu_reference_rate(flags, budget_s: float, max_steps: int):
     u0[0] = INFLOW_U
     lat.set_populations(O.feq_field(np.ones(SHAPE), u0))
     del u0
+    warmup = max(1, int(warmup))
     t = time.perf_counter()
-    lat.step(1)
-    first = time.perf_counter() - t
+    lat.step(warmup)
+    first = (time.perf_counter() - t) / warmup
     steps = int(max(1, min(max_steps, budget_s / max(first, 1e-6))))
     t = time.perf_counter()
     lat.step(steps)
     dt = time.perf_counter() - t
     n = SHAPE[0] * SHAPE[1] * SHAPE[2]
     rate = n * steps / dt / 1e9
-    sample = (f"{steps} steps (after 1 warm-up step) of the {SHAPE[0]}x{SHAPE[1]}x{SHAPE[2]} sphere "
+    sample = (f"{steps} steps (after {warmup} warm-up step{'s' if warmup > 1 else ''}) of the "
+              f"{SHAPE[0]}x{SHAPE[1]}x{SHAPE[2]} sphere "
               f"channel, f64 CPU oracle (reference operation order), OpenMP")
     return rate, threads, steps, dt, sample
 
@@ -266,7 +268,7 @@ def run_reference(args, rank: int):
         return
     flags = channel_geometry()
     budget = float(os.environ.get("LBM_REF_BUDGET_S", "30"))
-    rate, cores, steps, dt, sample = cpu_reference_rate(flags, budget, max(1, args.steps))
+    rate, cores, steps, dt, sample = cpu_reference_rate(flags, budget, max(1, args.steps), args.warmup)
     line = {
         "metric": METRIC,
         "value": rate,
@@ -274,7 +276,7 @@ def run_reference(args, rank: int):
         "impl": "reference",
         "n_gpus": args.gpus,
         "steps": steps,
-        "warmup": 1,
+        "warmup": max(1, args.warmup),
         "ms_per_step": dt / steps * 1e3,
         "higher_is_better": True,
         "scaling": "weak",
