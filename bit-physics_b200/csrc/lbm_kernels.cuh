@@ -674,8 +674,10 @@ __device__ __forceinline__ void rule_pair(const Params& P, const Streams<typenam
 // (z0, z0 + 1), then (z0 + 2, z0 + 3), and each direction leaves as one
 // 8-byte store.  Against the two-cell kernel a thread keeps twice the bytes in
 // flight per load phase and issues fewer instructions per cell: 78.6 against
-// 66.0 GLUPS (f16) on the 256x128x128 lattice without flags, the same results
-// bit for bit.  The quads that need a rule (3.7 % of the sphere channel's)
+// 66.0 GLUPS (f16) on the 256x128x128 lattice without flags.  The plain quads
+// collide their stored values with the storage shift folded into constants
+// (ModeFast::collide2s): within the storage's rounding of the two-cell
+// kernel, not bit for bit.  The quads that need a rule (3.7 % of the sphere channel's)
 // return from the plain path: there they would hold up their whole warp (the
 // rule quads sit in 23 % of the channel's rows), and their code would raise
 // the register demand of the plain path.  The first `rblocks` blocks of the

@@ -4,8 +4,9 @@ blocks the quads that need a boundary rule) on a B200.
 Lattices with many solid cells, walled faces, inflow / outflow planes and
 per-cell forces, stepped with the one-, two- and four-cell kernels mixed with
 readback steps, sums steps and the first step after an upload: the three
-give the same bits, and stay within tolerance of the oracle.  Slabs whose
-halo planes cut through spheres stay bit-identical to the unsplit lattice.
+agree within the storage tolerance and stay within tolerance of the oracle.
+Slabs whose halo planes cut through spheres stay bit-identical to the
+unsplit lattice.
 """
 
 from __future__ import annotations
