@@ -449,9 +449,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     import torch
 
     dist_on = world > 1
+    torch.cuda.set_device(local_rank)  # before the process group: each rank's NCCL communicator on its own GPU
     if dist_on:
         torch.distributed.init_process_group("nccl", timeout=timedelta(seconds=300))
-    torch.cuda.set_device(local_rank)
     dev = local_rank
     try:
         uuid = str(torch.cuda.get_device_properties(dev).uuid)
@@ -916,9 +916,9 @@ def run_slab(args, rank: int, world: int, local_rank: int):
     import torch
 
     dist_on = world > 1
+    torch.cuda.set_device(local_rank)  # before the process group: each rank's NCCL communicator on its own GPU
     if dist_on:
         torch.distributed.init_process_group("nccl", timeout=timedelta(seconds=300))
-    torch.cuda.set_device(local_rank)
     storage = args.storage
     n = int(np.prod(SHAPE))
     legs = {}
