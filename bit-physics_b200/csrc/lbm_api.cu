@@ -229,15 +229,29 @@ int refresh_rule_quads(lbm_lattice* h)
     CK(cudaMemcpyAsync(h->rule_counts, counts, sizeof(int) * QUAD_KINDS, cudaMemcpyDeviceToHost, h->stream),
        "rule quad counts");
     CK(cudaStreamSynchronize(h->stream), "rule quad sync");
-    // Leading blocks of k_step4: about 0.8 rule tasks per thread for each
+    // The lists come out in the order of the listing kernel's atomics; in
+    // lattice order, the consecutive tasks of a warp step neighbouring quads,
+    // whose gathers share cache lines.
+    std::vector<int> list;
+    for (int k = 0; k < QUAD_KINDS; ++k) {
+        if (h->rule_counts[k] < 2) continue;
+        int* dev = h->rule_quads + (size_t)k * cap;
+        list.resize(h->rule_counts[k]);
+        CK(cudaMemcpy(list.data(), dev, sizeof(int) * list.size(), cudaMemcpyDeviceToHost), "rule quad list");
+        std::sort(list.begin(), list.end());
+        CK(cudaMemcpy(dev, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice), "rule quad list");
+    }
+    // Leading blocks of k_step4: about 0.7 rule tasks per thread for each
     // wave of resident blocks (4 of 128 threads per SM) the plain quads take,
     // so that the rule blocks finish within the plain ones' time.  Sphere
-    // channel (23,930 rule quads): 35 blocks; measured 59.0 us at 32 and
-    // 59.5 at 36 (the plain quads alone: 59.3), 61.5 at 28, 66.1 at 24.
+    // channel (23,930 rule quads, f16): 38 blocks; measured 58.4 / 58.2 /
+    // 58.5 us at 32 / 36 / 40, 61.0 at 28, 66.1 at 24, 60.2 at 48.  The same
+    // spheres without inflow / outflow (19,834): 32 blocks, 57.5 us.
     const long long total = (long long)h->rule_counts[0] + h->rule_counts[1] + h->rule_counts[2];
     const long long plain = (long long)cap - total > 0 ? (long long)cap - total : 1;
-    const long long want = (2 * total * 5 * h->sms + plain - 1) / plain;
+    const long long want = (2 * total * 11 * h->sms + 2 * plain - 1) / (2 * plain);
     h->rules_grid = total > 0 ? (int)(want < 1 ? 1 : (want > 4 * h->sms ? 4 * h->sms : want)) : 0;
+    if (h->rules_grid_set > 0) h->rules_grid = h->rules_grid_set;
     h->params_version += 1;  // a captured step graph holds the old count
     return LBM_OK;
 }
@@ -900,6 +914,25 @@ int lbm_step_commit(lbm_lattice* h)
     h->cur ^= 1;
     h->steps += 1;
     h->open_step = false;
+    return LBM_OK;
+}
+
+int lbm_set_rule_blocks(lbm_lattice* h, int32_t blocks)
+{
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if ((rc = check_no_open_step(h))) return rc;
+    if (blocks < 0 || blocks > 65536) return fail(LBM_ERR_INVALID, "rule blocks must be in [0, 65536]");
+    if (h->vec != 4) return fail(LBM_ERR_STATE, "the lattice does not step four cells per thread");
+    h->rules_grid_set = blocks;
+    return refresh_rule_quads(h);
+}
+
+int lbm_get_rule_blocks(const lbm_lattice* h, int32_t* blocks, int32_t* rule_quads)
+{
+    if (!h) return fail(LBM_ERR_INVALID, "null lattice handle");
+    if (blocks) *blocks = h->rules_grid;
+    if (rule_quads) *rule_quads = h->rule_counts[0] + h->rule_counts[1] + h->rule_counts[2];
     return LBM_OK;
 }
 

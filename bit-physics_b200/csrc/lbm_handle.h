@@ -55,6 +55,7 @@ struct lbm_lattice {
     int* order = nullptr;       // Params::order of the plain one- / two-cell steps (walled lattices)
     int rule_counts[lbm::QUAD_KINDS] = {0, 0, 0};
     int rules_grid = 0;
+    int rules_grid_set = 0;     // lbm_set_rule_blocks (0: sized from the lists)
     int sms = 148;              // SMs of the lattice's device
     // Many steps per cooperative launch (LBM_STAGING_PERSISTENT): barrier
     // state, the limit of one barrier wait, and arrivals added to the

@@ -87,6 +87,8 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "lbm_step_count": ([_h], C.c_int64),
     "lbm_step_planes": ([_h, _i, _i], C.c_int),
     "lbm_step_commit": ([_h], C.c_int),
+    "lbm_set_rule_blocks": ([_h, _i], C.c_int),
+    "lbm_get_rule_blocks": ([_h, C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
     "lbm_get_rho_u": ([_h, _dp, _dp], C.c_int),
     "lbm_run_capture": ([_h, _i, _i, _dp, _dp], C.c_int),
     "lbm_step_monitor": ([_h, _i, _dp], C.c_int),

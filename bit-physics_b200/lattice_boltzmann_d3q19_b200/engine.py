@@ -212,6 +212,17 @@ class Lattice:
     def step_commit(self) -> None:
         N.check(N.lib().lbm_step_commit(self._h))
 
+    def set_rule_blocks(self, blocks: int = 0) -> None:
+        """Four-cell lattices: the number of leading blocks of each step launch
+        that step the quads needing a boundary rule (0: sized from their count)."""
+        N.check(N.lib().lbm_set_rule_blocks(self._h, int(blocks)))
+
+    def rule_blocks(self) -> tuple[int, int]:
+        """(leading blocks, rule quads) of a four-cell lattice."""
+        b, q = C.c_int32(), C.c_int32()
+        N.check(N.lib().lbm_get_rule_blocks(self._h, C.byref(b), C.byref(q)))
+        return b.value, q.value
+
     @property
     def step_count(self) -> int:
         return int(N.lib().lbm_step_count(self._h))

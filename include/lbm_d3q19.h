@@ -166,6 +166,14 @@ int64_t lbm_step_count(const lbm_lattice* h);
 int lbm_step_planes(lbm_lattice* h, int32_t x_begin, int32_t x_end);
 int lbm_step_commit(lbm_lattice* h);
 
+/* Four-cell lattices (16-bit storage, nz % 4 == 0): the quads that need a
+ * boundary rule are stepped by the leading blocks of each step launch.
+ * lbm_set_rule_blocks fixes their number (0: sized from the rule-quad count,
+ * the default); lbm_get_rule_blocks reports it and the number of rule quads.
+ * Results do not depend on it.  LBM_ERR_STATE for other lattices. */
+int lbm_set_rule_blocks(lbm_lattice* h, int32_t blocks);
+int lbm_get_rule_blocks(const lbm_lattice* h, int32_t* blocks, int32_t* rule_quads);
+
 /* rho and u of the current state: density_field + macroscopic_velocity
  * (d3q19_warp.py:283-292, :371-383).  Either pointer may be NULL. */
 int lbm_get_rho_u(lbm_lattice* h, double* rho, double* u);
