@@ -535,6 +535,15 @@ int lbm_create(const lbm_desc* desc, lbm_lattice** out)
                         bz = desc->nz / h->vec - 2 * (int)h->P.walled[2];
         const long long inner = bx > 0 && by > 0 && bz > 0 ? bx * by * bz : 0;
         if (faces != (long long)items - inner) return cleanup(fail(LBM_ERR_CUDA, "face order incomplete"));
+        if (faces > 1) {  // the face items into lattice order
+            std::vector<int> list(faces);
+            e = cudaMemcpy(list.data(), h->order, sizeof(int) * list.size(), cudaMemcpyDeviceToHost);
+            if (e == cudaSuccess) {
+                std::sort(list.begin(), list.end());
+                e = cudaMemcpy(h->order, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice);
+            }
+            if (e != cudaSuccess) return cleanup(cuda_fail(e, "face order"));
+        }
     }
     // Rest state f = w_i (rho = 1, u = 0).
     e = launch_feq_init(h->storage, h->P, nullptr, nullptr, h->buf[0], h->stream);

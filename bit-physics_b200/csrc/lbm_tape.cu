@@ -6,6 +6,7 @@
 // State s_k = the lattice buffer after k steps: s_0 = f_0 (PRE), s_k = P_{k-1}.
 // Memory: ceil(N / K) checkpoints + the final state + K - 1 segment states
 // + two adjoint fields + the special-cell list, all in one device allocation.
+#include <algorithm>
 #include <vector>
 
 #include "lbm_adjoint.cuh"
@@ -125,6 +126,15 @@ int lbm_tape_forward(lbm_lattice* h, int32_t n_steps, int32_t checkpoint_every, 
     e = launch_list_special(h->P, t->special, count, h->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&t->n_special, count, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e == cudaSuccess && t->n_special > 1) {
+        // into lattice order: neighbouring cells in a warp's consecutive tasks
+        std::vector<int> cells(t->n_special);
+        e = cudaMemcpy(cells.data(), t->special, sizeof(int) * cells.size(), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) {
+            std::sort(cells.begin(), cells.end());
+            e = cudaMemcpy(t->special, cells.data(), sizeof(int) * cells.size(), cudaMemcpyHostToDevice);
+        }
+    }
     if (e != cudaSuccess) {
         free_tape(t);
         return cuda_fail(e, "special-cell list");

@@ -17,7 +17,8 @@ import torch
 from adjoint_cases import case
 from gpu_cases import pair, random_state
 
-from lattice_boltzmann_d3q19_b200 import Lattice, geometry
+from lattice_boltzmann_d3q19_b200 import Lattice, LbmError, geometry
+from lattice_boltzmann_d3q19_b200 import _native as N
 from lattice_boltzmann_d3q19_b200.slab import SlabGroup, slab_bounds
 from test_gpu_slab import gpu_slab
 
@@ -151,3 +152,26 @@ def test_slabs_through_spheres_match_unsplit(storage):
     for s in group.slabs:
         s.engine.lat.close()
     assert np.array_equal(f, f_ref)
+
+
+def test_rule_block_count_does_not_change_results():
+    """The number of leading rule blocks of the four-cell kernel (automatic,
+    one, many) changes the schedule, not the populations."""
+    shape = (24, 16, 16)
+    flags, _ = geometry.sphere_channel(shape, n_spheres=3, radius=(2.0, 4.0), seed=5)
+    outs = []
+    for blocks in (0, 1, 7, 200):
+        with Lattice(shape, 0.56, storage="f16", inflow_u=(0.04, 0.0, 0.0)) as lat:
+            lat.set_flags(flags)
+            lat.set_rule_blocks(blocks)
+            b, q = lat.rule_blocks()
+            assert q > 0 and (b == blocks if blocks else b >= 1)
+            lat.set_equilibrium(1.0, (0.04, 0.0, 0.0))
+            lat.step(17)
+            outs.append(lat.get_populations())
+    for f in outs[1:]:
+        assert np.array_equal(f, outs[0])
+    with Lattice((8, 8, 6), 0.6, storage="f16") as lat:  # nz % 4 != 0: two cells per thread
+        with pytest.raises(LbmError) as e:
+            lat.set_rule_blocks(4)
+        assert e.value.code == N.LBM_ERR_STATE
