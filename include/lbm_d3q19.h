@@ -42,8 +42,9 @@ extern "C" {
 /* ---- storage formats of the population arrays on the device ------------ */
 #define LBM_STORAGE_F64 0        /* f64, reference operation order (bit-exact)   */
 #define LBM_STORAGE_F32 1        /* f32 populations, f32 arithmetic               */
-#define LBM_STORAGE_F16_SHIFT 2  /* binary16 (f_i - w_i), f32 arithmetic          */
-#define LBM_STORAGE_BF16_SHIFT 3 /* bfloat16 (f_i - w_i), f32 arithmetic          */
+#define LBM_STORAGE_F16_SHIFT 2  /* binary16 f_i - feq_i(1, storage_ref_u) (f_i - w_i
+                                    by default), f32 arithmetic                     */
+#define LBM_STORAGE_BF16_SHIFT 3 /* bfloat16, the same deviation, f32 arithmetic  */
 
 /* ---- periodicity bits; a non-periodic axis has two walled faces -------- */
 #define LBM_PERIODIC_X 1
