@@ -218,8 +218,9 @@ cudaError_t lbm::api::launch(lbm_lattice* h, int kernel, const void* src, void* 
 
 namespace {
 
-// The quads k_step4 leaves to k_step4_rules, from the current flags and
-// walled faces (four-cell lattices only).
+// The quads k_step4's plain path leaves to its leading blocks, from the
+// current flags and walled faces (four-cell lattices only), and the number
+// of those blocks.
 int refresh_rule_quads(lbm_lattice* h)
 {
     if (h->vec != 4) return LBM_OK;

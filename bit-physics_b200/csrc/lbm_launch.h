@@ -64,9 +64,9 @@ cudaError_t launch_load_f64(int storage, const Params& P, const void* src, doubl
 cudaError_t launch_feq_init(int storage, const Params& P, const double* rho, const double* u, void* dst,
                             cudaStream_t s);
 cudaError_t launch_mark_near_solid(const Params& P, uint8_t* flags, uint32_t* bbmask, cudaStream_t s);
-// The quads of a lattice (nz a multiple of 4) that k_step4 leaves to
-// k_step4_rules, by kind into lists + kind * cap; their numbers into
-// counts[QUAD_KINDS] (device).
+// The quads of a lattice (nz a multiple of 4) that k_step4's plain path
+// leaves to its leading blocks, by kind into lists + kind * cap (in no
+// order); their numbers into counts[QUAD_KINDS] (device).
 cudaError_t launch_list_rule_quads(const Params& P, int* lists, int cap, int* counts, cudaStream_t s);
 // Params::order for items of vec (1 or 2) cells; *face_count (device)
 // receives the number of items on the walled faces.
